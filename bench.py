@@ -1,0 +1,309 @@
+"""Benchmark: dedoppler Gsamples/s and % of the HBM roofline on one wide-band node.
+
+Workload ("node"): 64 coarse channels x 16 timesteps x 2^20 fine channels of float32
+power (4.3 GB), the same noise/bandpass model per coarse channel with independent seeds,
+4 drifting tones and 2 broadband spikes each; max_drift 4 Hz/s, snr_threshold 10.  One
+step searches all 64 coarse channels.  Inputs live in HBM before the timed region; the
+node is larger than L2, so consecutive coarse channels do not share cache.  Data are
+synthetic (seticore_b200.synthetic).
+
+`value` is the device-timed throughput (CUDA events, max over ranks); `e2e` is the same
+metric through the public API with the inputs in pinned host memory, so the host->device
+copy of every coarse channel is inside the timed region (copies overlap the previous
+channel's search on a second stream).  Multi-GPU runs are independent replicas (weak
+scaling): every rank searches its own node; nothing is exchanged.
+
+--impl reference times the reference's own CPU Taylor path (oracle/_ref/libref_cpu.so:
+the reference's taylorOneStepOneChannel over all channels, all host threads) on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_COARSE = 64
+T = 16
+N = 1 << 20
+MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
+METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
+UNIT = "Gsamples/s"
+# DRAM bytes per tree-kernel launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
+# ncu capture summarised in profiles/tree_max_kernel_node.md (None until captured).
+TREE_DRAM_BYTES = None
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes_fp32(Tr, n, ndb):
+    """Per search: one stats read, one tree read per drift block, a (sum, drift, offset)
+    write per channel: 4*Tr*N*(ndb+1) + 12*N."""
+    return 4 * Tr * n * (ndb + 1) + 12 * n
+
+
+def cpu_baseline(kind="reference", steps=1):
+    """The reference CPU Taylor path on one coarse channel of the node (bounded sample)."""
+    from oracle.oracle import Oracle, available
+    from seticore_b200.synthetic import config_node, make_filterbank_numpy
+    if kind == "reference" and not available("reference"):
+        kind = "port"
+    orc = Oracle(kind)
+    threads = orc.max_threads()
+    spec = config_node(1)[0]
+    x = make_filterbank_numpy(spec)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        orc.search(x, spec.foff_mhz, spec.tsamp, MAX_DRIFT, MIN_DRIFT, SNR)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.median(times))
+    value = spec.samples() / sec / 1e9
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"1 coarse channel (16 x 2^20, {spec.num_drift_blocks()} drift blocks), "
+                      f"{sec:.2f} s per search, median of {steps}"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        pass  # the CPU path has no warm-up state beyond the first call below
+    cb = cpu_baseline("reference", steps=max(1, args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "node: 64 coarse x 16 x 2^20 float32, max_drift 4 Hz/s, snr 10 "
+                                   "(CPU sample: 1 coarse channel per step)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import config_node, make_filterbank_torch
+
+    specs = config_node(N_COARSE, base_seed=2000 + 1000 * rank)
+    data = torch.empty((N_COARSE, T, N), dtype=torch.float32, device="cuda")
+    for i, s in enumerate(specs):
+        make_filterbank_torch(s, out=data[i])
+    torch.cuda.synchronize()
+    spec0 = specs[0]
+    dd = Dedopplerer(T, N, spec0.foff_mhz, spec0.tsamp)
+    stream = torch.cuda.current_stream()
+
+    tree_ms = []
+    hits_per_step = []
+
+    def step(record=False):
+        nh = 0
+        for i in range(N_COARSE):
+            hits = dd.search_raw(data[i], -1, i, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+            nh += len(hits)
+            if record:
+                tree_ms.append(dd.last_stats().tree_ms)
+        hits_per_step.append(nh)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(record=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+    samples_per_step = N_COARSE * T * N
+    value = world * samples_per_step / (ms / 1e3) / 1e9
+
+    # End to end through the public API: host (pinned) -> device copies inside the timing.
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((N_COARSE, T, N), dtype=torch.float32, pin_memory=True)
+        host.copy_(data)
+        bufs = [torch.empty((T, N), dtype=torch.float32, device="cuda") for _ in range(2)]
+        copy_stream = torch.cuda.Stream()
+        done = [torch.cuda.Event() for _ in range(2)]
+        freed = [torch.cuda.Event() for _ in range(2)]
+
+        def e2e_step():
+            with torch.cuda.stream(copy_stream):
+                bufs[0].copy_(host[0], non_blocking=True)
+                done[0].record(copy_stream)
+            nbytes = 0
+            for i in range(N_COARSE):
+                b = i % 2
+                if i + 1 < N_COARSE:
+                    nb = (i + 1) % 2
+                    with torch.cuda.stream(copy_stream):
+                        copy_stream.wait_event(freed[nb])
+                        bufs[nb].copy_(host[i + 1], non_blocking=True)
+                        done[nb].record(copy_stream)
+                stream.wait_event(done[b])
+                hits = dd.search_raw(bufs[b], -1, i, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+                freed[b].record(stream)
+                nbytes += 48 + 16 * 1024 + 40 * len(hits)
+            return nbytes
+
+        for f in freed:
+            f.record(stream)
+        e2e_step()
+        torch.cuda.synchronize()
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d2h = 0
+        for _ in range(e2e_steps):
+            d2h = e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world)
+        e2e = {"value": world * samples_per_step / (e_ms / 1e3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(host.numel() * 4), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e_ms}
+        del host
+
+    ndb = spec0.num_drift_blocks()
+    alg = algorithmic_bytes_fp32(T, N, ndb)
+    tree_avg_ms = float(np.mean(tree_ms))
+    peak, peak_src = measured_peak_hbm()
+    achieved = alg / (tree_avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": TREE_DRAM_BYTES, "peak_source": peak_src, "kernel": "tree_max_kernel<16,2,33>",
+                "kernel_ms": tree_avg_ms, "algorithmic_bytes_per_launch": alg,
+                "note": "algorithmic bytes assume one tree read per drift block; the fused kernel stages each "
+                        "input tile once for all drift blocks, so frac > 1 is expected"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "node: 64 coarse x 16 x 2^20 float32, 4 tones + 2 spikes per coarse channel, "
+                                   "max_drift 4 Hz/s, snr 10", "drift_blocks": ndb,
+                       "l2": "inputs (4.3 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
+            "clocks": clk, "roofline": roofline, "e2e": e2e,
+            "gpu_launches": len(tree_ms) * 9,
+            "hits_per_step": hits_per_step[-1]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline("reference", steps=1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dd.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

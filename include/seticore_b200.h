@@ -1,0 +1,115 @@
+/*
+ * seticore-b200: C ABI of the B200 dedoppler search.
+ *
+ * Every entry point returns an int status (SC_DD_OK on success) and never exits the
+ * process; sc_dd_last_error() gives the message of the calling thread's last failure.
+ * Pointers named dev_* are device-accessible (cudaMalloc'd, managed, or a view into a
+ * larger device buffer); other pointers are host memory.  Streams are cudaStream_t
+ * values passed as void*; NULL means the legacy default stream, which is the stream
+ * the reference runs everything on.
+ *
+ * Reference interface replaced (lacker/seticore 1.0.6):
+ *   class Dedopplerer, dedoppler.h:15-79 and dedoppler.cu:79-320.
+ * A header-only C++ class with the reference's signatures sits on top of this ABI in
+ * include/seticore_b200/dedoppler.hpp.
+ */
+#ifndef SETICORE_B200_H
+#define SETICORE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SC_DD_OK = 0,
+  SC_DD_EINVAL = 1,    /* bad argument (null pointer, T < 2, N < 64, window size 0) */
+  SC_DD_ECUDA = 2,     /* a CUDA runtime call failed */
+  SC_DD_ENOMEM = 3,    /* device or pinned allocation failed */
+  SC_DD_ETRUNC = 4,    /* more hits than the caller's capacity; *num_hits is the total */
+  SC_DD_EINTERNAL = 5, /* a device-side consistency check failed */
+  SC_DD_ESHAPE = 6     /* input shape differs from the engine's (dedoppler.cu:191-192) */
+};
+
+#define SC_DD_NO_BEAM (-1) /* dedoppler_hit.h:9 */
+
+/* One hit (dedoppler_hit.h:11-66 without the metadata-derived frequency). */
+typedef struct sc_dd_hit {
+  int index;              /* start channel within the coarse channel */
+  int drift_steps;        /* channels drifted over the rounded-up timesteps */
+  double drift_rate;      /* Hz/s: drift_steps * drift_rate_resolution */
+  float snr;              /* (power - median) / std_dev of the column sums */
+  float power;            /* the path sum */
+  float incoherent_power; /* filled by sc_dd_add_incoherent_power, else 0 */
+  int coarse_channel;
+  int beam;               /* the beam argument of the search */
+  int num_timesteps;      /* unrounded timesteps of the engine */
+} sc_dd_hit;
+
+/* Statistics of the last search (dedoppler.cu:322-354). */
+typedef struct sc_dd_stats {
+  float median;
+  float std_dev;
+  float mean;
+  float threshold;
+  int window_size;
+  int min_drift_block;
+  int max_drift_block;
+  int num_candidates; /* window maxima above threshold, before the min_drift filter */
+  float tree_ms;      /* device time of the Taylor-tree kernel(s), CUDA events on the stream */
+  float search_ms;    /* device time of the whole search, first memset to last kernel */
+} sc_dd_stats;
+
+typedef struct sc_dd sc_dd;
+
+/* Dedopplerer::Dedopplerer (dedoppler.cu:79-111).  num_timesteps is NOT rounded; the
+ * engine processes roundUpToPowerOfTwo(num_timesteps) rows.  Allocates all scratch. */
+int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double tsamp_s,
+                 int has_dc_spike, sc_dd** out);
+
+/* Dedopplerer::~Dedopplerer (dedoppler.cu:113-124). */
+int sc_dd_destroy(sc_dd* dd);
+
+/* Dedopplerer::memoryUsage (dedoppler.cu:127-130): device bytes the engine holds. */
+size_t sc_dd_memory_usage(const sc_dd* dd);
+
+/* Rounded timesteps (rows the input must have). */
+int sc_dd_rounded_timesteps(const sc_dd* dd);
+
+/* Dedopplerer::search (dedoppler.cu:186-320).  dev_input is [rounded T][N] row-major
+ * float32; row_stride is the element distance between rows (N for a dense buffer; a
+ * larger stride searches a window of a wider buffer in place).  Writes up to
+ * `capacity` hits in increasing index order and stores the total in *num_hits
+ * (SC_DD_ETRUNC when it exceeds capacity).  Work is ordered on `stream` after what
+ * is already queued there; the call returns once the hits are on the host. */
+int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int beam,
+                 int coarse_channel, double max_drift, double min_drift,
+                 double snr_threshold, sc_dd_hit* out, int capacity, int* num_hits,
+                 void* stream);
+
+/* Dedopplerer::addIncoherentPower (dedoppler.cu:139-176) for hits in place: each
+ * hit's incoherent_power becomes the path sum of dev_input along the hit's path.
+ * Unlike the reference this does not reorder the array (the C++ layer sorts by
+ * drift_steps first, as the reference does). */
+int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_stride,
+                               sc_dd_hit* hits, int num_hits, void* stream);
+
+/* Statistics of the engine's last completed search. */
+int sc_dd_last_stats(const sc_dd* dd, sc_dd_stats* out);
+
+/* Copies an internal per-channel array of the last search into dst (any memory
+ * cudaMemcpy can reach): which = 0 top path sums, 1 column sums.  N floats. */
+int sc_dd_copy_channel_array(sc_dd* dd, int which, float* dst, void* stream);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* sc_dd_last_error(void);
+
+/* Library version string. */
+const char* sc_dd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SETICORE_B200_H */

@@ -1,0 +1,98 @@
+"""ctypes binding of the C ABI in include/seticore_b200.h (libseticore_b200.so).
+
+The library is loaded from seticore_b200/_lib/ (built in-tree by seticore_b200.build).
+There is no fallback: if the library is missing, loading raises.
+"""
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libseticore_b200.so")
+
+SC_DD_OK = 0
+SC_DD_EINVAL = 1
+SC_DD_ECUDA = 2
+SC_DD_ENOMEM = 3
+SC_DD_ETRUNC = 4
+SC_DD_EINTERNAL = 5
+SC_DD_ESHAPE = 6
+NO_BEAM = -1
+
+# Every symbol the header declares; tests check the library exports all of them.
+EXPORTED = [
+    "sc_dd_create", "sc_dd_destroy", "sc_dd_memory_usage", "sc_dd_rounded_timesteps",
+    "sc_dd_search", "sc_dd_add_incoherent_power", "sc_dd_last_stats",
+    "sc_dd_copy_channel_array", "sc_dd_last_error", "sc_dd_version",
+]
+
+
+class ScDdHit(ctypes.Structure):
+    _fields_ = [
+        ("index", ctypes.c_int),
+        ("drift_steps", ctypes.c_int),
+        ("drift_rate", ctypes.c_double),
+        ("snr", ctypes.c_float),
+        ("power", ctypes.c_float),
+        ("incoherent_power", ctypes.c_float),
+        ("coarse_channel", ctypes.c_int),
+        ("beam", ctypes.c_int),
+        ("num_timesteps", ctypes.c_int),
+    ]
+
+
+class ScDdStats(ctypes.Structure):
+    _fields_ = [
+        ("median", ctypes.c_float),
+        ("std_dev", ctypes.c_float),
+        ("mean", ctypes.c_float),
+        ("threshold", ctypes.c_float),
+        ("window_size", ctypes.c_int),
+        ("min_drift_block", ctypes.c_int),
+        ("max_drift_block", ctypes.c_int),
+        ("num_candidates", ctypes.c_int),
+        ("tree_ms", ctypes.c_float),
+        ("search_ms", ctypes.c_float),
+    ]
+
+
+class DedopplerError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"seticore_b200 error {code}: {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} not found: build it with `python -m seticore_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d, ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+        L.sc_dd_create.argtypes = [i, i, d, d, i, ctypes.POINTER(vp)]
+        L.sc_dd_destroy.argtypes = [vp]
+        L.sc_dd_memory_usage.argtypes = [vp]
+        L.sc_dd_memory_usage.restype = ctypes.c_size_t
+        L.sc_dd_rounded_timesteps.argtypes = [vp]
+        L.sc_dd_search.argtypes = [vp, vp, ll, i, i, d, d, d, ctypes.POINTER(ScDdHit), i,
+                                   ctypes.POINTER(i), vp]
+        L.sc_dd_add_incoherent_power.argtypes = [vp, vp, ll, ctypes.POINTER(ScDdHit), i, vp]
+        L.sc_dd_last_stats.argtypes = [vp, ctypes.POINTER(ScDdStats)]
+        L.sc_dd_copy_channel_array.argtypes = [vp, i, vp, vp]
+        L.sc_dd_last_error.restype = ctypes.c_char_p
+        L.sc_dd_version.restype = ctypes.c_char_p
+        for name in EXPORTED:
+            getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int
+        L.sc_dd_last_error.restype = ctypes.c_char_p
+        L.sc_dd_version.restype = ctypes.c_char_p
+        L.sc_dd_memory_usage.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != SC_DD_OK:
+        raise DedopplerError(rc, lib().sc_dd_last_error().decode())
+    return rc

@@ -1,0 +1,265 @@
+"""Python host interface mirroring seticore's dedoppler API.
+
+Names, arguments and results follow the reference:
+  * FilterbankBuffer      -- filterbank_buffer.h:11-48 (row-major [time][channel] float32)
+  * FilterbankMetadata    -- filterbank_metadata.h:17-62 (the fields the search reads)
+  * DedopplerHit          -- dedoppler_hit.h:11-66, dedoppler_hit.cpp:11-73
+  * Dedopplerer           -- dedoppler.h:15-79 (search, addIncoherentPower, memoryUsage)
+
+Device memory is held in torch CUDA tensors and work is queued on torch's current CUDA
+stream; all arithmetic runs in the CUDA library through the C ABI.  There is no CPU
+path: a search on a tensor that is not on a CUDA device raises.
+"""
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+from . import _capi
+from ._capi import NO_BEAM, check, lib
+
+
+def roundUpToPowerOfTwo(n: int) -> int:  # util.cpp:16-22
+    r = 1
+    while r < n:
+        r *= 2
+    return r
+
+
+@dataclass
+class FilterbankMetadata:
+    """The metadata fields a search uses (filterbank_metadata.h:17-62)."""
+    fch1: float = 0.0
+    foff: float = 0.0  # MHz
+    tsamp: float = 0.0  # s
+    coarse_channel_size: int = 0
+    num_timesteps: int = 0
+    num_channels: int = 0
+    num_coarse_channels: int = 0
+    has_dc_spike: bool = False
+    source_name: str = ""
+    source_names: List[str] = field(default_factory=list)
+
+    def isCoherentBeam(self, beam: int) -> bool:  # filterbank_metadata.cpp:116-118
+        return 0 <= beam < len(self.source_names)
+
+
+@dataclass
+class DedopplerHit:
+    """dedoppler_hit.h:11-66."""
+    frequency: float
+    index: int
+    drift_steps: int
+    drift_rate: float
+    snr: float
+    coarse_channel: int
+    beam: int
+    num_timesteps: int
+    power: float
+    incoherent_power: float = 0.0
+
+    @classmethod
+    def make(cls, metadata: FilterbankMetadata, index, drift_steps, drift_rate, snr, beam,
+             coarse_channel, num_timesteps, power):
+        """The reference constructor (dedoppler_hit.cpp:11-23)."""
+        global_index = coarse_channel * metadata.coarse_channel_size + index
+        return cls(frequency=metadata.fch1 + global_index * metadata.foff, index=index,
+                   drift_steps=drift_steps, drift_rate=drift_rate, snr=snr,
+                   coarse_channel=coarse_channel,
+                   beam=beam if metadata.isCoherentBeam(beam) else NO_BEAM,
+                   num_timesteps=num_timesteps, power=power)
+
+    def toString(self) -> str:  # dedoppler_hit.cpp:25-30
+        bins = "bin" if self.drift_steps in (1, -1) else "bins"
+        return (f"coarse channel = {self.coarse_channel}, index = {self.index}, "
+                f"snr = {self.snr:.5f}, drift rate = {self.drift_rate:.5f} "
+                f"({self.drift_steps} {bins})")
+
+    def lowIndex(self) -> int:
+        return min(self.index, self.index + self.drift_steps)
+
+    def highIndex(self) -> int:
+        return max(self.index, self.index + self.drift_steps)
+
+    def expectedIndex(self, timesteps: int) -> int:  # dedoppler_hit.cpp:40-44
+        per = float(self.drift_steps) / float(self.num_timesteps - 1)
+        return self.index + int(_round_half_away(timesteps * per))
+
+    def score(self) -> float:  # dedoppler_hit.cpp:48-55
+        if self.incoherent_power > 0:
+            return self.power / self.incoherent_power
+        return -1.0 / (1.0 + self.snr)
+
+    def __lt__(self, other):  # dedoppler_hit.cpp:58-66
+        if self.coarse_channel != other.coarse_channel:
+            return self.coarse_channel < other.coarse_channel
+        if self.lowIndex() != other.lowIndex():
+            return self.lowIndex() < other.lowIndex()
+        return self.highIndex() < other.highIndex()
+
+
+def _round_half_away(x: float) -> float:
+    return math.floor(x + 0.5) if x >= 0 else -math.floor(-x + 0.5)
+
+
+def driftStepsLessThan(a: DedopplerHit, b: DedopplerHit) -> bool:  # dedoppler_hit.cpp:70-72
+    return a.drift_steps < b.drift_steps
+
+
+class FilterbankBuffer:
+    """Row-major [time][channel] float32 power on a CUDA device (filterbank_buffer.h).
+
+    FilterbankBuffer(T, N) allocates; FilterbankBuffer(T, N, data=tensor) is a view on an
+    existing CUDA tensor (a 2-D view with unit channel stride, e.g. one coarse channel
+    of a wider band: rows may be longer than N)."""
+
+    def __init__(self, num_timesteps: int, num_channels: int, data=None, device=None):
+        import torch
+        self.num_timesteps = num_timesteps
+        self.num_channels = num_channels
+        if data is None:
+            self.data = torch.zeros((num_timesteps, num_channels), dtype=torch.float32,
+                                    device=device or "cuda")
+            self.managed = True
+        else:
+            if data.dim() != 2 or data.shape[0] < num_timesteps or data.shape[1] < num_channels:
+                raise ValueError("FilterbankBuffer view has the wrong shape")
+            self.data = data
+            self.managed = False
+
+    @property
+    def row_stride(self) -> int:
+        return int(self.data.stride(0))
+
+    def zero(self):
+        self.data.zero_()
+
+    def set(self, time: int, channel: int, value: float):
+        self.data[time, channel] = value
+
+    def get(self, time: int, channel: int) -> float:
+        return float(self.data[time, channel])
+
+
+def makeNoisyBuffer(num_timesteps: int, num_channels: int, device=None) -> FilterbankBuffer:
+    """filterbank_buffer.cu:71-78: row 0 holds 0.1 * chan / N, everything else zero."""
+    import torch
+    buf = FilterbankBuffer(num_timesteps, num_channels, device=device)
+    buf.data[0] = 0.1 * torch.arange(num_channels, dtype=torch.float64, device=buf.data.device).float() / num_channels
+    return buf
+
+
+def _device_input(input, num_rows: int, num_channels: int):
+    import torch
+    t = input.data if isinstance(input, FilterbankBuffer) else input
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("dedoppler input must be a CUDA tensor or a FilterbankBuffer on a CUDA device")
+    if t.dtype != torch.float32 or t.dim() != 2 or t.stride(1) != 1:
+        raise TypeError("dedoppler input must be a 2-D float32 tensor with unit channel stride")
+    if t.shape[0] != num_rows or t.shape[1] != num_channels:
+        raise ValueError(f"input shape {tuple(t.shape)} != ({num_rows}, {num_channels}) "
+                         "(dedoppler.cu:191-192 requires rounded timesteps x channels)")
+    return t
+
+
+def _stream_handle(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+class Dedopplerer:
+    """The dedoppler search engine (dedoppler.h:15-79) on one CUDA device."""
+
+    def __init__(self, num_timesteps: int, num_channels: int, foff: float, tsamp: float,
+                 has_dc_spike: bool = False):
+        self.num_timesteps = num_timesteps
+        self.num_channels = num_channels
+        self.foff = foff
+        self.tsamp = tsamp
+        self.has_dc_spike = has_dc_spike
+        self.print_hits = False
+        self._h = ctypes.c_void_p()
+        check(lib().sc_dd_create(num_timesteps, num_channels, foff, tsamp, int(has_dc_spike),
+                                 ctypes.byref(self._h)))
+        self.rounded_num_timesteps = lib().sc_dd_rounded_timesteps(self._h)
+        self.drift_timesteps = self.rounded_num_timesteps - 1
+        self.drift_rate_resolution = 1e6 * foff / (self.drift_timesteps * tsamp)
+
+    def close(self):
+        if self._h:
+            lib().sc_dd_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def memoryUsage(self) -> int:
+        return int(lib().sc_dd_memory_usage(self._h))
+
+    def search_raw(self, input, beam: int, coarse_channel: int, max_drift: float,
+                   min_drift: float, snr_threshold: float, stream=None, capacity: int = 4096):
+        """Runs the search and returns the C ABI hit records (list of ScDdHit)."""
+        t = _device_input(input, self.rounded_num_timesteps, self.num_channels)
+        cap = capacity
+        while True:
+            buf = (_capi.ScDdHit * max(cap, 1))()
+            n = ctypes.c_int(0)
+            rc = lib().sc_dd_search(self._h, ctypes.c_void_p(t.data_ptr()), t.stride(0), beam,
+                                    coarse_channel, max_drift, min_drift, snr_threshold, buf, cap,
+                                    ctypes.byref(n), _stream_handle(stream))
+            if rc == _capi.SC_DD_ETRUNC:
+                cap = n.value
+                continue
+            check(rc)
+            return list(buf[: n.value])
+
+    def search(self, input, metadata: Optional[FilterbankMetadata], beam: int, coarse_channel: int,
+               max_drift: float, min_drift: float, snr_threshold: float,
+               output: Optional[list] = None, stream=None) -> list:
+        """Dedopplerer::search (dedoppler.cu:186-320); appends to `output` and returns it."""
+        if output is None:
+            output = []
+        meta = metadata or FilterbankMetadata(foff=self.foff, tsamp=self.tsamp,
+                                              coarse_channel_size=self.num_channels)
+        for h in self.search_raw(input, beam, coarse_channel, max_drift, min_drift, snr_threshold, stream):
+            hit = DedopplerHit.make(meta, h.index, h.drift_steps, h.drift_rate, h.snr, beam,
+                                    coarse_channel, self.num_timesteps, h.power)
+            if self.print_hits:
+                print("hit: " + hit.toString())
+            output.append(hit)
+        return output
+
+    def addIncoherentPower(self, input, hits: list, stream=None) -> None:
+        """Dedopplerer::addIncoherentPower (dedoppler.cu:139-176): sorts `hits` by
+        drift_steps (as the reference does) and fills incoherent_power."""
+        t = _device_input(input, self.rounded_num_timesteps, self.num_channels)
+        hits.sort(key=lambda h: h.drift_steps)
+        if not hits:
+            return
+        arr = (_capi.ScDdHit * len(hits))()
+        for i, h in enumerate(hits):
+            arr[i].index = h.index
+            arr[i].drift_steps = h.drift_steps
+        check(lib().sc_dd_add_incoherent_power(self._h, ctypes.c_void_p(t.data_ptr()), t.stride(0), arr,
+                                               len(hits), _stream_handle(stream)))
+        for i, h in enumerate(hits):
+            h.incoherent_power = arr[i].incoherent_power
+
+    add_incoherent_power = addIncoherentPower
+
+    def last_stats(self) -> _capi.ScDdStats:
+        s = _capi.ScDdStats()
+        check(lib().sc_dd_last_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def channel_array(self, which: str):
+        """Copy of the last search's per-channel 'top' path sums or 'colsum' column sums."""
+        import torch
+        out = torch.empty(self.num_channels, dtype=torch.float32, device="cuda")
+        check(lib().sc_dd_copy_channel_array(self._h, 0 if which == "top" else 1,
+                                             ctypes.c_void_p(out.data_ptr()), _stream_handle(None)))
+        return out
