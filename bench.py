@@ -174,6 +174,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--coarse", type=int, default=N_COARSE,
+                    help="coarse channels per node (64; fewer only for small profiling captures)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -187,8 +189,9 @@ def main():
     from seticore_b200 import Dedopplerer
     from seticore_b200.synthetic import config_node, make_filterbank_torch
 
-    specs = config_node(N_COARSE, base_seed=2000 + 1000 * rank)
-    data = torch.empty((N_COARSE, T, N), dtype=torch.float32, device="cuda")
+    n_coarse = args.coarse
+    specs = config_node(n_coarse, base_seed=2000 + 1000 * rank)
+    data = torch.empty((n_coarse, T, N), dtype=torch.float32, device="cuda")
     for i, s in enumerate(specs):
         make_filterbank_torch(s, out=data[i])
     torch.cuda.synchronize()
@@ -201,7 +204,7 @@ def main():
 
     def step(record=False):
         nh = 0
-        for i in range(N_COARSE):
+        for i in range(n_coarse):
             hits = dd.search_raw(data[i], -1, i, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
             nh += len(hits)
             if record:
@@ -223,13 +226,13 @@ def main():
     barrier(world)
     clk = clocks.stop()
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
-    samples_per_step = N_COARSE * T * N
+    samples_per_step = n_coarse * T * N
     value = world * samples_per_step / (ms / 1e3) / 1e9
 
     # End to end through the public API: host (pinned) -> device copies inside the timing.
     e2e = None
     if not args.no_e2e:
-        host = torch.empty((N_COARSE, T, N), dtype=torch.float32, pin_memory=True)
+        host = torch.empty((n_coarse, T, N), dtype=torch.float32, pin_memory=True)
         host.copy_(data)
         bufs = [torch.empty((T, N), dtype=torch.float32, device="cuda") for _ in range(2)]
         copy_stream = torch.cuda.Stream()
@@ -241,9 +244,9 @@ def main():
                 bufs[0].copy_(host[0], non_blocking=True)
                 done[0].record(copy_stream)
             nbytes = 0
-            for i in range(N_COARSE):
+            for i in range(n_coarse):
                 b = i % 2
-                if i + 1 < N_COARSE:
+                if i + 1 < n_coarse:
                     nb = (i + 1) % 2
                     with torch.cuda.stream(copy_stream):
                         copy_stream.wait_event(freed[nb])
@@ -289,11 +292,11 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "node: 64 coarse x 16 x 2^20 float32, 4 tones + 2 spikes per coarse channel, "
-                                   "max_drift 4 Hz/s, snr 10", "drift_blocks": ndb,
+            "config": {"workload": f"node: {n_coarse} coarse x 16 x 2^20 float32, 4 tones + 2 spikes per coarse "
+                                   "channel, max_drift 4 Hz/s, snr 10", "drift_blocks": ndb,
                        "l2": "inputs (4.3 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
             "clocks": clk, "roofline": roofline, "e2e": e2e,
-            "gpu_launches": len(tree_ms) * 9,
+            "gpu_launches": len(tree_ms) * 11,
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline("reference", steps=1)

@@ -64,6 +64,7 @@ struct sc_dd {
   scb::SelectState* sel = nullptr;
   scb::MomentPartial* partials = nullptr;
   int n_partials = 0;
+  double* var_scratch = nullptr;
   void* result = nullptr;  // SearchHeader followed by Candidate[cand_cap]
   int cand_cap = 0;
   float* scratch_a = nullptr;
@@ -91,6 +92,7 @@ void free_all(sc_dd* d) {
   cudaFree(d->colsum);
   cudaFree(d->sel);
   cudaFree(d->partials);
+  cudaFree(d->var_scratch);
   cudaFree(d->result);
   cudaFree(d->scratch_a);
   cudaFree(d->scratch_b);
@@ -166,6 +168,7 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
       (e = dalloc(d, &d->colsum, sizeof(float) * N)) != cudaSuccess ||
       (e = dalloc(d, &d->sel, sizeof(scb::SelectState))) != cudaSuccess ||
       (e = dalloc(d, &d->partials, sizeof(scb::MomentPartial) * d->n_partials)) != cudaSuccess ||
+      (e = dalloc(d, &d->var_scratch, sizeof(double) * 2 * scb::kVarChunks)) != cudaSuccess ||
       (e = dalloc(d, &d->result, result_bytes)) != cudaSuccess ||
       (d->Tr > 16 && (e = dalloc(d, &d->scratch_a, sizeof(float) * N * d->Tr)) != cudaSuccess) ||
       (d->Tr > 16 && (e = dalloc(d, &d->scratch_b, sizeof(float) * N * d->Tr)) != cudaSuccess) ||
@@ -229,7 +232,8 @@ int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int be
       (e = cudaMemsetAsync(dd->result, 0, sizeof(scb::SearchHeader), stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search: memset");
   if ((e = scb::search_stats(dev_input, row_stride, Tr, N, dd->colsum, dd->sel, dd->partials,
-                             dd->n_partials, snr_threshold, dd->hdr(), dd->num_sms, stream)) != cudaSuccess)
+                             dd->n_partials, dd->var_scratch, snr_threshold, dd->hdr(), dd->num_sms,
+                             stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search: statistics kernels");
   cudaEventRecord(dd->ev[1], stream);
   if (Tr <= 16) {
@@ -258,7 +262,8 @@ int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int be
                             dd->cands(), dd->cand_cap, dd->num_sms, stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search: hit kernels");
   cudaEventRecord(dd->ev[3], stream);
-  const size_t head = sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands;
+  const int head_cands = std::min(kHostCands, dd->cand_cap);
+  const size_t head = sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * head_cands;
   if ((e = cudaMemcpyAsync(dd->host_result, dd->result, head, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search: result copy");
@@ -268,10 +273,10 @@ int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int be
   std::vector<scb::Candidate> cands(ncand);
   const scb::Candidate* hc = reinterpret_cast<const scb::Candidate*>(
       static_cast<const char*>(dd->host_result) + sizeof(scb::SearchHeader));
-  std::copy(hc, hc + std::min(ncand, kHostCands), cands.begin());
-  if (ncand > kHostCands) {
-    if ((e = cudaMemcpyAsync(cands.data() + kHostCands, dd->cands() + kHostCands,
-                             sizeof(scb::Candidate) * (ncand - kHostCands), cudaMemcpyDeviceToHost,
+  std::copy(hc, hc + std::min(ncand, head_cands), cands.begin());
+  if (ncand > head_cands) {
+    if ((e = cudaMemcpyAsync(cands.data() + head_cands, dd->cands() + head_cands,
+                             sizeof(scb::Candidate) * (ncand - head_cands), cudaMemcpyDeviceToHost,
                              stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(stream)) != cudaSuccess)
       return cuda_fail(e, "sc_dd_search: candidate copy");

@@ -46,10 +46,18 @@ struct SelectState {
   uint32_t rank[3];
   unsigned ticket;
   unsigned hist[3][256];
+  // filled by moments_kernel for the variance kernels
+  float mean;
+  int pad;
+  long long n_lo, n_hi, n;
 };
 
+// Variance emulation scratch: per-chunk sums of the squared deviations and per-chunk
+// emulated contributions (kVarChunks entries each).
+constexpr int kVarChunks = 1024;
+
 struct MomentPartial {
-  double s1, s2;
+  double s1, s2;  // s2 unused (kept for layout)
   unsigned long long lt_first, eq_first, lt_last, eq_last;
 };
 
@@ -70,7 +78,7 @@ struct SearchHeader {
 };
 
 cudaError_t search_stats(const float* input, long long row_stride, int Tr, int N, float* colsum,
-                         SelectState* st, MomentPartial* partials, int n_partials,
+                         SelectState* st, MomentPartial* partials, int n_partials, double* var_scratch,
                          double snr_threshold, SearchHeader* hdr, int num_sms, cudaStream_t stream);
 
 // Window de-duplication (dedoppler.cu:353-383) and drift recovery of the survivors.

@@ -6,14 +6,21 @@
 //   * colsum_kernel: sumColumns (dedoppler.cu:63-72), same sequential float order.
 //   * select_pass (x4): MSB-first radix select of the three order statistics at once,
 //     8 bits per pass; the last CTA of each pass picks the digits.  Exact.
-//   * moments_kernel: sum and sum of squares (FP64) of the values between the two
-//     percentiles, with boundary ties counted exactly; per-CTA partials are combined
-//     by the last CTA in a fixed order, so the result does not depend on scheduling.
-//     It then forms mean, standard deviation and threshold with the reference's float
-//     roundings (float mean from the rounded sum; float sqrt; float threshold).
-// The reference accumulates the variance in float over an nth_element-permuted order;
-// the FP64 sum here differs from it only by that float rounding (about 1e-5 relative
-// at 2^20 channels).
+//   * moments_kernel: the sum (FP64, as the reference's std::accumulate with a double
+//     start) of the values between the two percentiles, with boundary ties counted
+//     exactly; per-CTA partials are combined by the last CTA in a fixed order.  It forms
+//     the mean with the reference's roundings (float sum, float division).
+//   * var_chunk_kernel + var_emulate_kernel: the variance.  The reference accumulates
+//     (f - m)^2 in FLOAT, one term at a time (dedoppler.cu:337-341).  Once the
+//     accumulator is large, every term is rounded to the accumulator's ulp and terms
+//     under half an ulp vanish, which biases the sum low (about 4e-4 relative at 2^20
+//     channels, nearly independent of the order).  An exact FP64 variance would
+//     therefore differ from the reference's by more than the SNR tolerance.  These two
+//     kernels reproduce the float accumulation in parallel: an exact prefix sum gives
+//     the accumulator A_i each term meets (in channel order), and the term contributes
+//     rint(t_i / ulp(float(A_i))) * ulp(float(A_i)).  The result tracks a sequential
+//     float sum to about 1e-5 relative; the remaining difference comes from the order
+//     (the reference's order is whatever std::nth_element leaves).
 #include "dd_common.cuh"
 #include "dd_internal.h"
 
@@ -119,7 +126,6 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
     const float f = x[i];
     if (f > v_first && f < v_last) {
       acc.s1 += (double)f;
-      acc.s2 += (double)f * (double)f;
     }
     acc.lt_first += (f < v_first);
     acc.eq_first += (f == v_first);
@@ -129,7 +135,6 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
   // Warp then block reduction in a fixed order.
   for (int o = 16; o > 0; o >>= 1) {
     acc.s1 += __shfl_down_sync(0xffffffffu, acc.s1, o);
-    acc.s2 += __shfl_down_sync(0xffffffffu, acc.s2, o);
     acc.lt_first += __shfl_down_sync(0xffffffffu, acc.lt_first, o);
     acc.eq_first += __shfl_down_sync(0xffffffffu, acc.eq_first, o);
     acc.lt_last += __shfl_down_sync(0xffffffffu, acc.lt_last, o);
@@ -142,7 +147,6 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
     MomentPartial b = red[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
       b.s1 += red[w].s1;
-      b.s2 += red[w].s2;
       b.lt_first += red[w].lt_first;
       b.eq_first += red[w].eq_first;
       b.lt_last += red[w].lt_last;
@@ -159,7 +163,6 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
   for (int b = 0; b < (int)gridDim.x; ++b) {
     const MomentPartial q = partials[b];
     t.s1 += q.s1;
-    t.s2 += q.s2;
     t.lt_first += q.lt_first;
     t.eq_first += q.eq_first;
     t.lt_last += q.lt_last;
@@ -167,10 +170,9 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
   }
   st->ticket = 0;
   const long long n = (long long)last - first + 1;
-  double s1, s2;
+  double s1;
   if (v_first == v_last) {
     s1 = (double)n * v_first;
-    s2 = (double)n * (double)v_first * (double)v_first;
   } else {
     // Sorted positions holding v_first are [lt_first, lt_first + eq_first - 1], those
     // holding v_last are [lt_last, lt_last + eq_last - 1]; count the ones in [first, last].
@@ -178,24 +180,157 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
     const long long n_lo = lo_end - first + 1;
     const long long n_hi = (long long)last - max((long long)t.lt_last, (long long)first) + 1;
     s1 = t.s1 + (double)n_lo * v_first + (double)n_hi * v_last;
-    s2 = t.s2 + (double)n_lo * (double)v_first * (double)v_first + (double)n_hi * (double)v_last * (double)v_last;
   }
   const float sum_f = (float)s1;
-  const float m = sum_f / (float)n;  // dedoppler.cu:336: float sum / count
-  const double md = (double)m;
-  const double accum = s2 - 2.0 * md * s1 + (double)n * md * md;
-  const float accum_f = (float)(accum > 0.0 ? accum : 0.0);
-  const float std_dev = sqrtf(accum_f / (float)n);
+  const float m = sum_f / (float)n;  // dedoppler.cu:335-336: float sum / count
   hdr->median = v_mid;
   hdr->mean = m;
+  st->mean = m;
+  st->n = n;
+  if (v_first == v_last) {
+    st->n_lo = n;
+    st->n_hi = 0;
+  } else {
+    const long long lo_end = min((long long)t.lt_first + (long long)t.eq_first - 1, (long long)last);
+    st->n_lo = lo_end - first + 1;
+    st->n_hi = (long long)last - max((long long)t.lt_last, (long long)first) + 1;
+  }
+}
+
+
+__device__ __forceinline__ double float_ulp_above(double a) {
+  const float af = __double2float_rn(a);
+  if (af <= 0.0f) return 1.401298464324817e-45;  // 2^-149: the first add is exact
+  return (double)(__uint_as_float(__float_as_uint(af) + 1u) - af);
+}
+
+// The squared deviation the reference adds: (f - m) * (f - m) in float.
+__device__ __forceinline__ float var_term(float f, float m) {
+  const float d = f - m;
+  return __fmul_rn(d, d);
+}
+
+__device__ __forceinline__ bool var_inside(float f, float lo, float hi) { return f > lo && f < hi; }
+
+// Per-chunk exact sums of the terms of the channels strictly between the percentiles.
+__global__ void var_chunk_kernel(const float* __restrict__ x, int N, const SelectState* st, int chunk,
+                                 double* chunk_sum) {
+  __shared__ double red[32];
+  const float lo = key_float(st->prefix[0]), hi = key_float(st->prefix[2]);
+  const float m = st->mean;
+  const long long b0 = (long long)blockIdx.x * chunk;
+  const long long b1 = min((long long)N, b0 + chunk);
+  double acc = 0.0;
+  for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const float f = x[i];
+    if (var_inside(f, lo, hi)) acc += (double)var_term(f, m);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += red[w];
+    chunk_sum[blockIdx.x] = b;
+  }
+}
+
+// Exclusive block scan of one double per thread (blockDim.x <= 1024, multiple of 32).
+__device__ double block_exclusive_scan(double v, double* warp_tot, double* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    double w = (lane < nw) ? warp_tot[lane] : 0.0;
+    double wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < nw) warp_tot[lane] = wi - w;  // exclusive prefix of the warp totals
+    if (lane == nw - 1) *total = wi;
+  }
+  __syncthreads();
+  const double r = warp_tot[warp] + (inc - v);
+  __syncthreads();
+  return r;
+}
+
+// Emulates the float accumulation over every included term, in channel order, then the
+// boundary copies; the last CTA forms the standard deviation and the threshold.
+__global__ void var_emulate_kernel(const float* __restrict__ x, int N, SelectState* st, int chunk,
+                                   const double* chunk_sum, double* chunk_part, double snr_threshold,
+                                   SearchHeader* hdr) {
+  __shared__ double warp_tot[32];
+  __shared__ double tile_total;
+  __shared__ double red[32];
+  __shared__ bool last_block;
+  const float lo = key_float(st->prefix[0]), hi = key_float(st->prefix[2]);
+  const float m = st->mean;
+  double base = 0.0;
+  for (int b = 0; b < (int)blockIdx.x; ++b) base += chunk_sum[b];
+  const long long b0 = (long long)blockIdx.x * chunk;
+  const long long b1 = min((long long)N, b0 + chunk);
+  double contrib = 0.0;
+  for (long long t0 = b0; t0 < b1; t0 += blockDim.x) {
+    const long long i = t0 + threadIdx.x;
+    double term = 0.0;
+    if (i < b1) {
+      const float f = x[i];
+      if (var_inside(f, lo, hi)) term = (double)var_term(f, m);
+    }
+    const double pre = block_exclusive_scan(term, warp_tot, &tile_total);
+    if (term != 0.0) {
+      const double u = float_ulp_above(base + pre);
+      contrib += rint(term / u) * u;
+    }
+    base += tile_total;
+  }
+  for (int o = 16; o > 0; o >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = contrib;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += red[w];
+    chunk_part[blockIdx.x] = c;
+    __threadfence();
+    last_block = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last_block || threadIdx.x != 0) return;
+  __threadfence();
+  double acc = 0.0, exact = 0.0;
+  for (int b = 0; b < (int)gridDim.x; ++b) {
+    acc += __ldcg(chunk_part + b);
+    exact += __ldcg(chunk_sum + b);
+  }
+  // The percentile values themselves (ties at the boundaries), added after the rest.
+  const double tlo = (double)var_term(lo, m), thi = (double)var_term(hi, m);
+  for (long long k = 0; k < st->n_lo + st->n_hi; ++k) {
+    const double term = (k < st->n_lo) ? tlo : thi;
+    if (term != 0.0) {
+      const double u = float_ulp_above(exact);
+      acc += rint(term / u) * u;
+    }
+    exact += term;
+  }
+  st->ticket = 0;
+  const float accum_f = (float)acc;
+  const float std_dev = sqrtf(accum_f / (float)st->n);  // dedoppler.cu:342
   hdr->std_dev = std_dev;
-  hdr->threshold = (float)(snr_threshold * (double)std_dev + (double)v_mid);  // dedoppler.cu:353
+  hdr->threshold = (float)(snr_threshold * (double)std_dev + (double)hdr->median);  // dedoppler.cu:353
 }
 
 }  // namespace
 
 cudaError_t search_stats(const float* input, long long row_stride, int Tr, int N, float* colsum,
-                         SelectState* st, MomentPartial* partials, int n_partials,
+                         SelectState* st, MomentPartial* partials, int n_partials, double* var_scratch,
                          double snr_threshold, SearchHeader* hdr, int num_sms, cudaStream_t stream) {
   const int first = (int)ceil(0.05 * N);
   const int last = (int)floor(0.95 * N);
@@ -208,6 +343,14 @@ cudaError_t search_stats(const float* input, long long row_stride, int Tr, int N
   for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<sblocks, 256, 0, stream>>>(colsum, N, st, shift);
   int mblocks = sblocks < n_partials ? sblocks : n_partials;
   moments_kernel<<<mblocks, 256, 0, stream>>>(colsum, N, st, first, last, snr_threshold, partials, hdr);
+  int vchunks = 2 * num_sms;
+  if (vchunks > kVarChunks) vchunks = kVarChunks;
+  if (vchunks > (N + 255) / 256) vchunks = (N + 255) / 256;
+  const int chunk = (N + vchunks - 1) / vchunks;
+  vchunks = (N + chunk - 1) / chunk;
+  var_chunk_kernel<<<vchunks, 256, 0, stream>>>(colsum, N, st, chunk, var_scratch);
+  var_emulate_kernel<<<vchunks, 256, 0, stream>>>(colsum, N, st, chunk, var_scratch, var_scratch + kVarChunks,
+                                                  snr_threshold, hdr);
   return cudaGetLastError();
 }
 
