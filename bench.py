@@ -36,8 +36,8 @@ MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per tree-kernel launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
-# ncu capture summarised in profiles/tree_max_kernel_node.md (None until captured).
-TREE_DRAM_BYTES = None
+# ncu capture summarised in profiles/tree_max_kernel_node.md.
+TREE_DRAM_BYTES = 71950848
 
 
 def dist_setup():
