@@ -29,7 +29,8 @@ enum {
   SC_DD_ENOMEM = 3,    /* device or pinned allocation failed */
   SC_DD_ETRUNC = 4,    /* more hits than the caller's capacity; *num_hits is the total */
   SC_DD_EINTERNAL = 5, /* a device-side consistency check failed */
-  SC_DD_ESHAPE = 6     /* input shape differs from the engine's (dedoppler.cu:191-192) */
+  SC_DD_ESHAPE = 6,    /* input shape differs from the engine's (dedoppler.cu:191-192) */
+  SC_DD_ELIMIT = 7     /* a size exceeds the stated maximum of sc_dd_search_static */
 };
 
 #define SC_DD_NO_BEAM (-1) /* dedoppler_hit.h:9 */
@@ -107,6 +108,37 @@ const char* sc_dd_last_error(void);
 
 /* Library version string. */
 const char* sc_dd_version(void);
+
+/* Largest channel count sc_dd_search_static accepts. */
+#define SC_DD_STATIC_MAX_CHANNELS 1048576
+
+/* The search, for callers that cannot allocate device memory where they search -- e.g. a
+ * real-time capture or beamforming pipeline that reserved the GPU's memory up front and
+ * must not call cudaMalloc (which can synchronise the device) in its processing loop, or a
+ * host framework whose allocator owns all device memory.  No counterpart in the
+ * reference; it has no engine object.
+ *
+ * Same inputs, results and ordering as sc_dd_search, plus the shape (unrounded
+ * num_timesteps, num_channels, foff in MHz, tsamp in s) that sc_dd_create would take.
+ * It calls no cudaMalloc, cudaFree, cudaMallocHost or other allocating routine: its scratch
+ * is one fixed device array inside the library (about 9.2 MB, held by every GPU that loads
+ * the library until the process exits) and its host side uses the stack and `out`.
+ * Limits (SC_DD_ELIMIT beyond them): num_channels <= SC_DD_STATIC_MAX_CHANNELS, rounded
+ * timesteps <= 16, at most 65536 windows (num_channels / window_size).  Errors are status
+ * codes only (sc_dd_last_error is not updated).
+ *
+ * The array is shared by every call on a device and keeps the last call's contents; each
+ * call clears what must start at zero.  Calls that overlap on the GPU -- on different
+ * streams, or from different host threads -- race on it and must be serialised by the
+ * caller.  The first call on each device looks up the array's device address (with that
+ * device current) and caches it; make that first call before any stream capture.  On
+ * SC_DD_ETRUNC, *num_hits is the total and the hits written are not necessarily the
+ * lowest-index ones. */
+int sc_dd_search_static(const float* dev_input, long long row_stride, int num_timesteps,
+                        int num_channels, double foff_mhz, double tsamp_s, int beam,
+                        int coarse_channel, double max_drift, double min_drift,
+                        double snr_threshold, sc_dd_hit* out, int capacity, int* num_hits,
+                        void* stream);
 
 #ifdef __cplusplus
 }
