@@ -35,8 +35,9 @@ N = 1 << 20
 MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
-# DRAM bytes per tree-kernel launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
-# ncu capture summarised in profiles/tree_max_kernel_node.md.
+# DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from the ncu capture summarised in profiles/tree_max_kernel_node.md;
+# a launch covering k coarse channels moves k times this.
 TREE_DRAM_BYTES = 71950848
 
 
@@ -201,15 +202,15 @@ def main():
 
     tree_ms = []
     hits_per_step = []
+    inputs = [data[i] for i in range(n_coarse)]
+    beams = [-1] * n_coarse
+    coarse = list(range(n_coarse))
 
     def step(record=False):
-        nh = 0
-        for i in range(n_coarse):
-            hits = dd.search_raw(data[i], -1, i, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
-            nh += len(hits)
-            if record:
-                tree_ms.append(dd.last_stats().tree_ms)
-        hits_per_step.append(nh)
+        res = dd.search_batch_raw(inputs, beams, coarse, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+        if record:
+            tree_ms.append(dd.last_stats().tree_ms)
+        hits_per_step.append(sum(len(h) for h in res))
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -229,33 +230,40 @@ def main():
     samples_per_step = n_coarse * T * N
     value = world * samples_per_step / (ms / 1e3) / 1e9
 
-    # End to end through the public API: host (pinned) -> device copies inside the timing.
+    # End to end through the public API: host (pinned) -> device copies inside the timing,
+    # in chunks of E2E_CHUNK coarse channels; the copy of chunk j+1 overlaps the search of j.
     e2e = None
     if not args.no_e2e:
+        E2E_CHUNK = 8
         host = torch.empty((n_coarse, T, N), dtype=torch.float32, pin_memory=True)
         host.copy_(data)
-        bufs = [torch.empty((T, N), dtype=torch.float32, device="cuda") for _ in range(2)]
+        bufs = [torch.empty((E2E_CHUNK, T, N), dtype=torch.float32, device="cuda") for _ in range(2)]
         copy_stream = torch.cuda.Stream()
         done = [torch.cuda.Event() for _ in range(2)]
         freed = [torch.cuda.Event() for _ in range(2)]
+        chunks = [(j, min(E2E_CHUNK, n_coarse - j)) for j in range(0, n_coarse, E2E_CHUNK)]
+
+        def issue_copy(ci):
+            j, m = chunks[ci]
+            b = ci % 2
+            with torch.cuda.stream(copy_stream):
+                copy_stream.wait_event(freed[b])
+                bufs[b][:m].copy_(host[j:j + m], non_blocking=True)
+                done[b].record(copy_stream)
 
         def e2e_step():
-            with torch.cuda.stream(copy_stream):
-                bufs[0].copy_(host[0], non_blocking=True)
-                done[0].record(copy_stream)
             nbytes = 0
-            for i in range(n_coarse):
-                b = i % 2
-                if i + 1 < n_coarse:
-                    nb = (i + 1) % 2
-                    with torch.cuda.stream(copy_stream):
-                        copy_stream.wait_event(freed[nb])
-                        bufs[nb].copy_(host[i + 1], non_blocking=True)
-                        done[nb].record(copy_stream)
+            issue_copy(0)
+            for ci, (j, m) in enumerate(chunks):
+                b = ci % 2
+                if ci + 1 < len(chunks):
+                    issue_copy(ci + 1)
                 stream.wait_event(done[b])
-                hits = dd.search_raw(bufs[b], -1, i, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+                res = dd.search_batch_raw([bufs[b][k] for k in range(m)], [-1] * m, list(range(j, j + m)),
+                                          MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
                 freed[b].record(stream)
-                nbytes += 48 + 16 * 1024 + 40 * len(hits)
+                # headers + first candidates of each search come back in two copies per call
+                nbytes += m * (32 + 24 * 256)
             return nbytes
 
         for f in freed:
@@ -279,13 +287,16 @@ def main():
         del host
 
     ndb = spec0.num_drift_blocks()
-    alg = algorithmic_bytes_fp32(T, N, ndb)
-    tree_avg_ms = float(np.mean(tree_ms))
+    per_launch = min(n_coarse, 64)
+    alg = algorithmic_bytes_fp32(T, N, ndb) * per_launch
+    # tree_ms times the one tree-kernel launch that covers the first (up to) 64 searches
+    tree_launch_ms = float(np.mean(tree_ms))
     peak, peak_src = measured_peak_hbm()
-    achieved = alg / (tree_avg_ms / 1e3) / 1e9
+    achieved = alg / (tree_launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": TREE_DRAM_BYTES, "peak_source": peak_src, "kernel": "tree_max_kernel<16,2,33>",
-                "kernel_ms": tree_avg_ms, "algorithmic_bytes_per_launch": alg,
+                "traffic": (TREE_DRAM_BYTES * per_launch if TREE_DRAM_BYTES else None), "peak_source": peak_src,
+                "kernel": "tree_max_kernel<16,2,33>", "searches_per_launch": per_launch,
+                "kernel_ms": tree_launch_ms, "algorithmic_bytes_per_launch": alg,
                 "note": "algorithmic bytes assume one tree read per drift block; the fused kernel stages each "
                         "input tile once for all drift blocks, so frac > 1 is expected"}
 
@@ -296,7 +307,7 @@ def main():
                                    "channel, max_drift 4 Hz/s, snr 10", "drift_blocks": ndb,
                        "l2": "inputs (4.3 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
             "clocks": clk, "roofline": roofline, "e2e": e2e,
-            "gpu_launches": len(tree_ms) * 11,
+            "gpu_launches": len(tree_ms) * 12 * ((n_coarse + 63) // 64),
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline("reference", steps=1)

@@ -89,6 +89,20 @@ int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int be
                  double snr_threshold, sc_dd_hit* out, int capacity, int* num_hits,
                  void* stream);
 
+/* Dedopplerer::search (dedoppler.cu:186-320) for `count` inputs of the engine's shape at
+ * once -- e.g. every coarse channel of a band or every beam -- sharing max_drift,
+ * min_drift and snr_threshold.  Search k reads dev_inputs[k] with row_strides[k] and
+ * reports beams[k] / coarse_channels[k].  Up to 64 searches share each launch of every
+ * kernel, and the hits come back with one synchronisation per 64 searches.  Hits are
+ * written search after search (each search's in increasing index order); num_hits[k]
+ * receives search k's count.  The engine keeps scratch for the largest batch it has run
+ * (the first call with a larger count, up to 64, allocates more). */
+int sc_dd_search_batch(sc_dd* dd, int count, const float* const* dev_inputs,
+                       const long long* row_strides, const int* beams,
+                       const int* coarse_channels, double max_drift, double min_drift,
+                       double snr_threshold, sc_dd_hit* out, int capacity, int* num_hits,
+                       void* stream);
+
 /* Dedopplerer::addIncoherentPower (dedoppler.cu:139-176) for hits in place: each
  * hit's incoherent_power becomes the path sum of dev_input along the hit's path.
  * Unlike the reference this does not reorder the array (the C++ layer sorts by
@@ -96,7 +110,8 @@ int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int be
 int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_stride,
                                sc_dd_hit* hits, int num_hits, void* stream);
 
-/* Statistics of the engine's last completed search. */
+/* Statistics of the first search of the engine's last completed call; tree_ms and
+ * search_ms time its first batch of up to 64 searches. */
 int sc_dd_last_stats(const sc_dd* dd, sc_dd_stats* out);
 
 /* Copies an internal per-channel array of the last search into dst (any memory

@@ -22,7 +22,7 @@ NO_BEAM = -1
 # Every symbol the header declares; tests check the library exports all of them.
 EXPORTED = [
     "sc_dd_create", "sc_dd_destroy", "sc_dd_memory_usage", "sc_dd_rounded_timesteps",
-    "sc_dd_search", "sc_dd_add_incoherent_power", "sc_dd_last_stats",
+    "sc_dd_search", "sc_dd_search_batch", "sc_dd_add_incoherent_power", "sc_dd_last_stats",
     "sc_dd_copy_channel_array", "sc_dd_last_error", "sc_dd_version", "sc_dd_search_static",
 ]
 
@@ -80,6 +80,9 @@ def lib():
         L.sc_dd_rounded_timesteps.argtypes = [vp]
         L.sc_dd_search.argtypes = [vp, vp, ll, i, i, d, d, d, ctypes.POINTER(ScDdHit), i,
                                    ctypes.POINTER(i), vp]
+        L.sc_dd_search_batch.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(ll), ctypes.POINTER(i),
+                                         ctypes.POINTER(i), d, d, d, ctypes.POINTER(ScDdHit), i,
+                                         ctypes.POINTER(i), vp]
         L.sc_dd_add_incoherent_power.argtypes = [vp, vp, ll, ctypes.POINTER(ScDdHit), i, vp]
         L.sc_dd_last_stats.argtypes = [vp, ctypes.POINTER(ScDdStats)]
         L.sc_dd_search_static.argtypes = [vp, ll, i, i, d, d, i, i, d, d, d, ctypes.POINTER(ScDdHit), i,

@@ -2,12 +2,16 @@
 //
 // sc_dd mirrors the reference's Dedopplerer (dedoppler.h:15-79): it is built for one
 // (timesteps, channels, foff, tsamp) shape and owns every scratch buffer, reused across
-// searches (dedoppler.cu:76-111).  A search queues, on the caller's stream:
-//   memset(top) -> column sums + order statistics + moments (dd_stats.cu)
-//   -> fused tree/top kernel (dd_tree.cu, or the level path of dd_levels.cu for Tr > 16)
+// searches (dedoppler.cu:76-111).  It keeps one scratch "slot" per search of the largest
+// batch it has run.  A call queues, on the caller's stream, for up to kMaxBatch searches
+// at a time:
+//   memset(top, headers) -> column sums + order statistics + variance (dd_stats.cu)
+//   -> fused tree/top kernel over every search's work items (dd_tree.cu; for Tr > 16 the
+//      level path of dd_levels.cu, one search at a time)
 //   -> window de-duplication + drift recovery (dd_hits.cu)
-// and then copies one small block (statistics + candidates) to pinned host memory.
-// Only the hit list crosses to the host, not the reference's four N-length arrays.
+// then copies the headers and the first candidates of every search to pinned host memory
+// in two copies and synchronises once.  Only hit lists cross to the host, not the
+// reference's four N-length arrays per search.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -32,7 +36,7 @@ int cuda_fail(cudaError_t err, const char* what) {
   return fail(SC_DD_ECUDA, std::string(what) + ": " + cudaGetErrorString(err));
 }
 
-constexpr int kHostCands = 1024;
+constexpr int kHostCands = 256;  // candidates per search fetched with the headers
 
 int round_up_pow2(int n) {  // util.cpp:16-22
   int r = 1;
@@ -52,6 +56,24 @@ struct DeviceGuard {
   }
 };
 
+// The drift range and window of a search (dedoppler.cu:165-167, 274-278, 354).
+struct DriftPlan {
+  double res;
+  int dmin, dmax, window_size;
+};
+
+DriftPlan plan_drift(int Tr, double foff, double tsamp, double max_drift) {
+  DriftPlan p;
+  const int drift_timesteps = Tr - 1;
+  p.res = 1e6 * foff / (drift_timesteps * tsamp);
+  const double diag = p.res * drift_timesteps;
+  const double nmax = max_drift / std::fabs(diag);
+  p.dmin = (int)std::floor(-nmax);
+  p.dmax = (int)std::floor(nmax);
+  p.window_size = (int)(2 * std::ceil(nmax * drift_timesteps));
+  return p;
+}
+
 }  // namespace
 
 struct sc_dd {
@@ -59,50 +81,36 @@ struct sc_dd {
   double foff = 0, tsamp = 0;
   int has_dc_spike = 0;
   int device = 0, num_sms = 148;
+  int n_partials = 0;
+  // Per-slot scratch, slot k at offset k * (per-slot size) in each array.
+  int slots = 0;
+  int cand_cap = 0;  // candidates per slot
   float* top = nullptr;
   float* colsum = nullptr;
   scb::SelectState* sel = nullptr;
   scb::MomentPartial* partials = nullptr;
-  int n_partials = 0;
-  double* var_scratch = nullptr;
-  void* result = nullptr;  // SearchHeader followed by Candidate[cand_cap]
-  int cand_cap = 0;
-  float* scratch_a = nullptr;
+  double* var = nullptr;
+  scb::SearchHeader* hdrs = nullptr;
+  scb::Candidate* cands = nullptr;
+  float* scratch_a = nullptr;  // Tr > 16 level buffers (one search at a time)
   float* scratch_b = nullptr;
-  void* host_result = nullptr;  // pinned: SearchHeader + kHostCands candidates
+  void* host = nullptr;  // pinned: slots * (header + kHostCands candidates)
   int* inc_index = nullptr;
   int* inc_steps = nullptr;
   float* inc_vals = nullptr;
   int inc_cap = 0;
   size_t device_bytes = 0;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // search start, tree start/end, search end
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, tree start/end, call end
   sc_dd_stats last{};
   bool have_last = false;
 
-  scb::SearchHeader* hdr() { return static_cast<scb::SearchHeader*>(result); }
-  scb::Candidate* cands() {
-    return reinterpret_cast<scb::Candidate*>(static_cast<char*>(result) + sizeof(scb::SearchHeader));
+  scb::SearchHeader* host_hdrs() { return static_cast<scb::SearchHeader*>(host); }
+  scb::Candidate* host_cands() {
+    return reinterpret_cast<scb::Candidate*>(static_cast<char*>(host) + sizeof(scb::SearchHeader) * slots);
   }
 };
 
 namespace {
-
-void free_all(sc_dd* d) {
-  cudaFree(d->top);
-  cudaFree(d->colsum);
-  cudaFree(d->sel);
-  cudaFree(d->partials);
-  cudaFree(d->var_scratch);
-  cudaFree(d->result);
-  cudaFree(d->scratch_a);
-  cudaFree(d->scratch_b);
-  cudaFree(d->inc_index);
-  cudaFree(d->inc_steps);
-  cudaFree(d->inc_vals);
-  if (d->host_result) cudaFreeHost(d->host_result);
-  for (cudaEvent_t& e : d->ev)
-    if (e) cudaEventDestroy(e);
-}
 
 template <typename T>
 cudaError_t dalloc(sc_dd* d, T** p, size_t bytes) {
@@ -111,12 +119,74 @@ cudaError_t dalloc(sc_dd* d, T** p, size_t bytes) {
   return e;
 }
 
+template <typename T>
+void dfree(sc_dd* d, T** p, size_t bytes) {
+  if (*p) {
+    cudaFree(*p);
+    d->device_bytes -= bytes;
+    *p = nullptr;
+  }
+}
+
+void free_slots(sc_dd* d) {
+  const size_t N = d->N, S = d->slots;
+  dfree(d, &d->top, sizeof(float) * N * S);
+  dfree(d, &d->colsum, sizeof(float) * N * S);
+  dfree(d, &d->sel, sizeof(scb::SelectState) * S);
+  dfree(d, &d->partials, sizeof(scb::MomentPartial) * d->n_partials * S);
+  dfree(d, &d->var, sizeof(double) * 2 * scb::kVarChunks * S);
+  dfree(d, &d->hdrs, sizeof(scb::SearchHeader) * S);
+  dfree(d, &d->cands, sizeof(scb::Candidate) * d->cand_cap * S);
+  if (d->host) cudaFreeHost(d->host);
+  d->host = nullptr;
+  d->slots = 0;
+}
+
+void free_all(sc_dd* d) {
+  free_slots(d);
+  dfree(d, &d->scratch_a, sizeof(float) * (size_t)d->N * d->Tr);
+  dfree(d, &d->scratch_b, sizeof(float) * (size_t)d->N * d->Tr);
+  dfree(d, &d->inc_index, sizeof(int) * d->inc_cap);
+  dfree(d, &d->inc_steps, sizeof(int) * d->inc_cap);
+  dfree(d, &d->inc_vals, sizeof(float) * d->inc_cap);
+  for (cudaEvent_t& e : d->ev)
+    if (e) cudaEventDestroy(e);
+}
+
+// Makes room for `slots` searches with `cand_cap` candidates each (never shrinks).
+int ensure_slots(sc_dd* d, int slots, int cand_cap) {
+  if (slots <= d->slots && cand_cap <= d->cand_cap) return SC_DD_OK;
+  const int ns = std::max(slots, d->slots);
+  const int nc = std::max(cand_cap, d->cand_cap);
+  cudaDeviceSynchronize();  // the old slots may still be in use by queued work
+  free_slots(d);
+  d->cand_cap = nc;
+  const size_t N = d->N, S = ns;
+  cudaError_t e;
+  if ((e = dalloc(d, &d->top, sizeof(float) * N * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->colsum, sizeof(float) * N * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->sel, sizeof(scb::SelectState) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->partials, sizeof(scb::MomentPartial) * d->n_partials * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->var, sizeof(double) * 2 * scb::kVarChunks * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->hdrs, sizeof(scb::SearchHeader) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->cands, sizeof(scb::Candidate) * (size_t)nc * S)) != cudaSuccess ||
+      (e = cudaMallocHost(&d->host, (sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands) * S)) !=
+          cudaSuccess) {
+    d->slots = ns;
+    free_slots(d);
+    return fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA,
+                std::string("scratch allocation failed: ") + cudaGetErrorString(e));
+  }
+  d->slots = ns;
+  if ((e = cudaMemset(d->sel, 0, sizeof(scb::SelectState) * S)) != cudaSuccess) return cuda_fail(e, "scratch memset");
+  return SC_DD_OK;
+}
+
 int ensure_inc(sc_dd* d, int n) {
   if (n <= d->inc_cap) return SC_DD_OK;
-  cudaFree(d->inc_index);
-  cudaFree(d->inc_steps);
-  cudaFree(d->inc_vals);
-  d->device_bytes -= (size_t)d->inc_cap * 12;
+  dfree(d, &d->inc_index, sizeof(int) * d->inc_cap);
+  dfree(d, &d->inc_steps, sizeof(int) * d->inc_cap);
+  dfree(d, &d->inc_vals, sizeof(float) * d->inc_cap);
   d->inc_cap = 0;
   const int cap = std::max(n, 4096);
   cudaError_t e;
@@ -128,16 +198,178 @@ int ensure_inc(sc_dd* d, int n) {
   return SC_DD_OK;
 }
 
+scb::SearchDesc make_desc(sc_dd* d, int slot, const float* input, long long row_stride, const DriftPlan& p,
+                          double snr_threshold) {
+  scb::SearchDesc s{};
+  const size_t N = d->N;
+  s.input = input;
+  s.row_stride = row_stride;
+  s.Tr = d->Tr;
+  s.N = d->N;
+  s.dmin = p.dmin;
+  s.dmax = p.dmax;
+  s.window_size = p.window_size;
+  s.first = (int)std::ceil(0.05 * d->N);  // dedoppler.cu:327
+  s.mid = d->N / 2;                        // dedoppler.cu:291
+  s.last = (int)std::floor(0.95 * d->N);  // dedoppler.cu:328
+  s.snr_threshold = snr_threshold;
+  s.top = d->top + N * slot;
+  s.colsum = d->colsum + N * slot;
+  s.sel = d->sel + slot;
+  s.partials = d->partials + (size_t)d->n_partials * slot;
+  s.var = d->var + (size_t)2 * scb::kVarChunks * slot;
+  s.hdr = d->hdrs + slot;
+  s.cands = d->cands + (size_t)d->cand_cap * slot;
+  s.cand_cap = d->cand_cap;
+  return s;
+}
+
+// Queues n <= kMaxBatch searches into slots 0..n-1.
+int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* strides, const DriftPlan& p,
+                double snr_threshold, cudaStream_t stream, bool first_batch) {
+  scb::SearchBatch b;
+  b.count = n;
+  b.maxN = dd->N;
+  for (int k = 0; k < n; ++k) b.s[k] = make_desc(dd, k, inputs[k], strides[k], p, snr_threshold);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(dd->top, 0, sizeof(float) * dd->N * (size_t)n, stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(dd->hdrs, 0, sizeof(scb::SearchHeader) * n, stream)) != cudaSuccess)
+    return cuda_fail(e, "memset");
+  if ((e = scb::search_stats_batch(b, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "statistics kernels");
+  if (first_batch) cudaEventRecord(dd->ev[1], stream);
+  if (dd->Tr <= 16) {
+    scb::TreeBatch tb;
+    tb.count = n;
+    tb.n_items = 0;
+    for (int k = 0; k < n; ++k) {
+      scb::TreeGroup& g = tb.g[k];
+      g = scb::TreeGroup{};
+      g.rows = inputs[k];
+      g.row_stride = strides[k];
+      g.job_row_stride = 0;
+      g.N = dd->N;
+      g.d_first = p.dmin;
+      g.d_step = 1;
+      g.n_jobs = p.dmax - p.dmin + 1;
+      g.db_first = p.dmin;
+      g.db_step = 1;
+      g.off_base = 0;
+      g.off_step = 0;
+      g.elig_T1 = dd->Tr - 1;
+      g.top = b.s[k].top;
+    }
+    e = scb::tree_max_batch(tb, dd->Tr, dd->num_sms, stream);
+  } else {
+    e = cudaSuccess;
+    for (int k = 0; k < n && e == cudaSuccess; ++k)
+      e = scb::levels_search(inputs[k], strides[k], dd->Tr, dd->N, p.dmin, p.dmax, dd->scratch_a, dd->scratch_b,
+                             b.s[k].top, dd->num_sms, stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "tree kernels");
+  if (first_batch) cudaEventRecord(dd->ev[2], stream);
+  if ((e = scb::search_hits_batch(b, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "hit kernels");
+  return SC_DD_OK;
+}
+
+// Runs `count` searches; hits of search k land in out[off_k ...], off_k = sum of earlier counts.
+int run_searches(sc_dd* dd, int count, const float* const* inputs, const long long* strides, const int* beams,
+                 const int* coarse, double max_drift, double min_drift, double snr_threshold, sc_dd_hit* out,
+                 int capacity, int* num_hits, cudaStream_t stream) {
+  const int Tr = dd->Tr, N = dd->N;
+  const DriftPlan p = plan_drift(Tr, dd->foff, dd->tsamp, max_drift);
+  if (!(p.window_size >= 1) || p.dmax < p.dmin)
+    return fail(SC_DD_EINVAL, "max_drift gives no drift range (window size < 1)");
+  if ((long long)(p.dmax - p.dmin + 1) * Tr > (1ll << 30)) return fail(SC_DD_EINVAL, "drift range too large");
+  const long long nwin = ((long long)N + p.window_size - 1) / p.window_size;
+  int rc = ensure_slots(dd, std::min(count, scb::kMaxBatch), (int)std::min<long long>(nwin + 1, N / 2 + 2));
+  if (rc != SC_DD_OK) return rc;
+  cudaError_t e;
+  if ((e = cudaEventRecord(dd->ev[0], stream)) != cudaSuccess) return cuda_fail(e, "event");
+  int total = 0;
+  for (int k0 = 0; k0 < count; k0 += scb::kMaxBatch) {
+    const int n = std::min(scb::kMaxBatch, count - k0);
+    rc = queue_batch(dd, n, inputs + k0, strides + k0, p, snr_threshold, stream, k0 == 0);
+    if (rc != SC_DD_OK) return rc;
+    if (k0 == 0) cudaEventRecord(dd->ev[3], stream);
+    // Headers of all n searches, then the first kHostCands candidates of each (strided copy).
+    const int head = std::min(kHostCands, dd->cand_cap);
+    if ((e = cudaMemcpyAsync(dd->host_hdrs(), dd->hdrs, sizeof(scb::SearchHeader) * n, cudaMemcpyDeviceToHost,
+                             stream)) != cudaSuccess ||
+        (e = cudaMemcpy2DAsync(dd->host_cands(), sizeof(scb::Candidate) * kHostCands, dd->cands,
+                               sizeof(scb::Candidate) * dd->cand_cap, sizeof(scb::Candidate) * head, n,
+                               cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+      return cuda_fail(e, "result copy");
+    for (int k = 0; k < n; ++k) {
+      const scb::SearchHeader h = dd->host_hdrs()[k];
+      const int ncand = std::min(h.num_candidates, dd->cand_cap);
+      std::vector<scb::Candidate> cands(ncand);
+      const scb::Candidate* hc = dd->host_cands() + (size_t)kHostCands * k;
+      std::copy(hc, hc + std::min(ncand, head), cands.begin());
+      if (ncand > head) {
+        if ((e = cudaMemcpyAsync(cands.data() + head, dd->cands + (size_t)dd->cand_cap * k + head,
+                                 sizeof(scb::Candidate) * (ncand - head), cudaMemcpyDeviceToHost, stream)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(stream)) != cudaSuccess)
+          return cuda_fail(e, "candidate copy");
+      }
+      std::sort(cands.begin(), cands.end(),
+                [](const scb::Candidate& a, const scb::Candidate& b) { return a.index < b.index; });
+      if (k0 + k == 0) {
+        dd->last.median = h.median;
+        dd->last.std_dev = h.std_dev;
+        dd->last.mean = h.mean;
+        dd->last.threshold = h.threshold;
+        dd->last.window_size = p.window_size;
+        dd->last.min_drift_block = p.dmin;
+        dd->last.max_drift_block = p.dmax;
+        dd->last.num_candidates = ncand;
+      }
+      int nk = 0;
+      for (const scb::Candidate& c : cands) {
+        int drift_bins = 0;
+        if (!scb::decode_candidate(c, p.dmin, Tr, &drift_bins))
+          return fail(SC_DD_EINTERNAL, "drift recovery did not reproduce a top sum");
+        // dedoppler.cu:385-396
+        const double drift_rate = drift_bins * p.res;
+        const float snr = (c.power - h.median) / h.std_dev;
+        if (std::fabs(drift_rate) >= min_drift) {
+          if (total < capacity) {
+            sc_dd_hit& o = out[total];
+            o.index = c.index;
+            o.drift_steps = drift_bins;
+            o.drift_rate = drift_rate;
+            o.snr = snr;
+            o.power = c.power;
+            o.incoherent_power = 0.0f;
+            o.coarse_channel = coarse[k0 + k];
+            o.beam = beams[k0 + k];
+            o.num_timesteps = dd->T;
+          }
+          ++total;
+          ++nk;
+        }
+      }
+      num_hits[k0 + k] = nk;
+    }
+  }
+  cudaEventElapsedTime(&dd->last.tree_ms, dd->ev[1], dd->ev[2]);
+  cudaEventElapsedTime(&dd->last.search_ms, dd->ev[0], dd->ev[3]);
+  dd->have_last = true;
+  if (total > capacity) return fail(SC_DD_ETRUNC, "more hits than capacity");
+  return SC_DD_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 const char* sc_dd_last_error(void) { return g_last_error.c_str(); }
 
-const char* sc_dd_version(void) { return "seticore-b200 0.1 (dedoppler; reference seticore 1.0.6)"; }
+const char* sc_dd_version(void) { return "seticore-b200 0.2 (dedoppler; reference seticore 1.0.6)"; }
 
-int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double tsamp_s,
-                 int has_dc_spike, sc_dd** out) {
+int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double tsamp_s, int has_dc_spike,
+                 sc_dd** out) {
   g_last_error.clear();
   if (!out) return fail(SC_DD_EINVAL, "sc_dd_create: out is null");
   *out = nullptr;
@@ -160,31 +392,20 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
     delete d;
     return cuda_fail(e, "sc_dd_create: no CUDA device");
   }
-  const size_t N = (size_t)num_channels;
-  d->n_partials = 4 * d->num_sms;
-  d->cand_cap = num_channels / 2 + 2;
-  const size_t result_bytes = sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * d->cand_cap;
-  if ((e = dalloc(d, &d->top, sizeof(float) * N)) != cudaSuccess ||
-      (e = dalloc(d, &d->colsum, sizeof(float) * N)) != cudaSuccess ||
-      (e = dalloc(d, &d->sel, sizeof(scb::SelectState))) != cudaSuccess ||
-      (e = dalloc(d, &d->partials, sizeof(scb::MomentPartial) * d->n_partials)) != cudaSuccess ||
-      (e = dalloc(d, &d->var_scratch, sizeof(double) * 2 * scb::kVarChunks)) != cudaSuccess ||
-      (e = dalloc(d, &d->result, result_bytes)) != cudaSuccess ||
-      (d->Tr > 16 && (e = dalloc(d, &d->scratch_a, sizeof(float) * N * d->Tr)) != cudaSuccess) ||
-      (d->Tr > 16 && (e = dalloc(d, &d->scratch_b, sizeof(float) * N * d->Tr)) != cudaSuccess) ||
-      (e = cudaMallocHost(&d->host_result,
-                          sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands)) != cudaSuccess) {
-    free_all(d);
-    delete d;
-    return fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA,
-                std::string("sc_dd_create: allocation failed: ") + cudaGetErrorString(e));
+  d->n_partials = 2 * d->num_sms;
+  // One slot; candidates for windows of 16 channels or more (grown when a call needs more).
+  int rc = ensure_slots(d, 1, std::min(num_channels / 2 + 2, num_channels / 16 + 2));
+  if (rc == SC_DD_OK && d->Tr > 16) {
+    if ((e = dalloc(d, &d->scratch_a, sizeof(float) * (size_t)num_channels * d->Tr)) != cudaSuccess ||
+        (e = dalloc(d, &d->scratch_b, sizeof(float) * (size_t)num_channels * d->Tr)) != cudaSuccess)
+      rc = fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA, "sc_dd_create: level buffers");
   }
-  e = cudaMemset(d->sel, 0, sizeof(scb::SelectState));
-  for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&d->ev[i]);
-  if (e != cudaSuccess) {
+  for (int i = 0; i < 4 && rc == SC_DD_OK; ++i)
+    if ((e = cudaEventCreate(&d->ev[i])) != cudaSuccess) rc = cuda_fail(e, "sc_dd_create: event");
+  if (rc != SC_DD_OK) {
     free_all(d);
     delete d;
-    return cuda_fail(e, "sc_dd_create: memset");
+    return rc;
   }
   *out = d;
   return SC_DD_OK;
@@ -202,129 +423,36 @@ size_t sc_dd_memory_usage(const sc_dd* dd) { return dd ? dd->device_bytes : 0; }
 
 int sc_dd_rounded_timesteps(const sc_dd* dd) { return dd ? dd->Tr : 0; }
 
-int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int beam,
-                 int coarse_channel, double max_drift, double min_drift, double snr_threshold,
-                 sc_dd_hit* out, int capacity, int* num_hits, void* stream_ptr) {
+int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int beam, int coarse_channel,
+                 double max_drift, double min_drift, double snr_threshold, sc_dd_hit* out, int capacity,
+                 int* num_hits, void* stream) {
   g_last_error.clear();
-  if (!dd || !dev_input || !num_hits || (capacity > 0 && !out))
-    return fail(SC_DD_EINVAL, "sc_dd_search: null argument");
+  if (!dd || !dev_input || !num_hits || (capacity > 0 && !out)) return fail(SC_DD_EINVAL, "sc_dd_search: null argument");
   if (row_stride < dd->N) return fail(SC_DD_ESHAPE, "sc_dd_search: row_stride smaller than num_channels");
   DeviceGuard guard(dd->device);
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  const int Tr = dd->Tr, N = dd->N;
-
-  // dedoppler.cu:165-167 and 274-278, 354: the same double arithmetic.
-  const int drift_timesteps = Tr - 1;
-  const double res = 1e6 * dd->foff / (drift_timesteps * dd->tsamp);
-  const double diag = res * drift_timesteps;
-  const double nmax = max_drift / std::fabs(diag);
-  const int dmin = (int)std::floor(-nmax);
-  const int dmax = (int)std::floor(nmax);
-  const int window_size = (int)(2 * std::ceil(nmax * drift_timesteps));
-  if (!(window_size >= 1) || dmax < dmin)
-    return fail(SC_DD_EINVAL, "sc_dd_search: max_drift gives no drift range (window size < 1)");
-  if ((long long)(dmax - dmin + 1) * Tr > (1ll << 30))
-    return fail(SC_DD_EINVAL, "sc_dd_search: drift range too large");
-
-  cudaError_t e;
-  if ((e = cudaEventRecord(dd->ev[0], stream)) != cudaSuccess) return cuda_fail(e, "sc_dd_search: event");
-  if ((e = cudaMemsetAsync(dd->top, 0, sizeof(float) * N, stream)) != cudaSuccess ||
-      (e = cudaMemsetAsync(dd->result, 0, sizeof(scb::SearchHeader), stream)) != cudaSuccess)
-    return cuda_fail(e, "sc_dd_search: memset");
-  if ((e = scb::search_stats(dev_input, row_stride, Tr, N, dd->colsum, dd->sel, dd->partials,
-                             dd->n_partials, dd->var_scratch, snr_threshold, dd->hdr(), dd->num_sms,
-                             stream)) != cudaSuccess)
-    return cuda_fail(e, "sc_dd_search: statistics kernels");
-  cudaEventRecord(dd->ev[1], stream);
-  if (Tr <= 16) {
-    scb::TreeParams tp{};
-    tp.rows = dev_input;
-    tp.row_stride = row_stride;
-    tp.job_row_stride = 0;
-    tp.N = N;
-    tp.d_first = dmin;
-    tp.d_step = 1;
-    tp.n_jobs = dmax - dmin + 1;
-    tp.db_first = dmin;
-    tp.db_step = 1;
-    tp.off_base = 0;
-    tp.off_step = 0;
-    tp.elig_T1 = Tr - 1;
-    tp.top = dd->top;
-    e = scb::tree_max(tp, Tr, dd->num_sms, stream);
-  } else {
-    e = scb::levels_search(dev_input, row_stride, Tr, N, dmin, dmax, dd->scratch_a, dd->scratch_b, dd->top,
-                           dd->num_sms, stream);
-  }
-  if (e != cudaSuccess) return cuda_fail(e, "sc_dd_search: tree kernels");
-  cudaEventRecord(dd->ev[2], stream);
-  if ((e = scb::search_hits(dev_input, row_stride, Tr, N, dd->top, window_size, dmin, dmax, dd->hdr(),
-                            dd->cands(), dd->cand_cap, dd->num_sms, stream)) != cudaSuccess)
-    return cuda_fail(e, "sc_dd_search: hit kernels");
-  cudaEventRecord(dd->ev[3], stream);
-  const int head_cands = std::min(kHostCands, dd->cand_cap);
-  const size_t head = sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * head_cands;
-  if ((e = cudaMemcpyAsync(dd->host_result, dd->result, head, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(stream)) != cudaSuccess)
-    return cuda_fail(e, "sc_dd_search: result copy");
-  const scb::SearchHeader h = *static_cast<scb::SearchHeader*>(dd->host_result);
-  if (h.error) return fail(SC_DD_EINTERNAL, "sc_dd_search: drift recovery did not reproduce a top sum");
-  const int ncand = std::min(h.num_candidates, dd->cand_cap);
-  std::vector<scb::Candidate> cands(ncand);
-  const scb::Candidate* hc = reinterpret_cast<const scb::Candidate*>(
-      static_cast<const char*>(dd->host_result) + sizeof(scb::SearchHeader));
-  std::copy(hc, hc + std::min(ncand, head_cands), cands.begin());
-  if (ncand > head_cands) {
-    if ((e = cudaMemcpyAsync(cands.data() + head_cands, dd->cands() + head_cands,
-                             sizeof(scb::Candidate) * (ncand - head_cands), cudaMemcpyDeviceToHost,
-                             stream)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(stream)) != cudaSuccess)
-      return cuda_fail(e, "sc_dd_search: candidate copy");
-  }
-  std::sort(cands.begin(), cands.end(),
-            [](const scb::Candidate& a, const scb::Candidate& b) { return a.index < b.index; });
-
-  dd->last.median = h.median;
-  dd->last.std_dev = h.std_dev;
-  dd->last.mean = h.mean;
-  dd->last.threshold = h.threshold;
-  dd->last.window_size = window_size;
-  dd->last.min_drift_block = dmin;
-  dd->last.max_drift_block = dmax;
-  dd->last.num_candidates = ncand;
-  cudaEventElapsedTime(&dd->last.tree_ms, dd->ev[1], dd->ev[2]);
-  cudaEventElapsedTime(&dd->last.search_ms, dd->ev[0], dd->ev[3]);
-  dd->have_last = true;
-
-  int n = 0;
-  for (const scb::Candidate& c : cands) {
-    // dedoppler.cu:385-396
-    const int drift_bins = c.drift_steps;
-    const double drift_rate = drift_bins * res;
-    const float snr = (c.power - h.median) / h.std_dev;
-    if (std::fabs(drift_rate) >= min_drift) {
-      if (n < capacity) {
-        sc_dd_hit& o = out[n];
-        o.index = c.index;
-        o.drift_steps = drift_bins;
-        o.drift_rate = drift_rate;
-        o.snr = snr;
-        o.power = c.power;
-        o.incoherent_power = 0.0f;
-        o.coarse_channel = coarse_channel;
-        o.beam = beam;
-        o.num_timesteps = dd->T;
-      }
-      ++n;
-    }
-  }
-  *num_hits = n;
-  if (n > capacity) return fail(SC_DD_ETRUNC, "sc_dd_search: more hits than capacity");
-  return SC_DD_OK;
+  return run_searches(dd, 1, &dev_input, &row_stride, &beam, &coarse_channel, max_drift, min_drift, snr_threshold,
+                      out, capacity, num_hits, static_cast<cudaStream_t>(stream));
 }
 
-int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_stride,
-                               sc_dd_hit* hits, int num_hits, void* stream_ptr) {
+int sc_dd_search_batch(sc_dd* dd, int count, const float* const* dev_inputs, const long long* row_strides,
+                       const int* beams, const int* coarse_channels, double max_drift, double min_drift,
+                       double snr_threshold, sc_dd_hit* out, int capacity, int* num_hits, void* stream) {
+  g_last_error.clear();
+  if (!dd || count < 0 || (count > 0 && (!dev_inputs || !row_strides || !beams || !coarse_channels || !num_hits)) ||
+      (capacity > 0 && !out))
+    return fail(SC_DD_EINVAL, "sc_dd_search_batch: null argument");
+  for (int k = 0; k < count; ++k) {
+    if (!dev_inputs[k]) return fail(SC_DD_EINVAL, "sc_dd_search_batch: null input");
+    if (row_strides[k] < dd->N) return fail(SC_DD_ESHAPE, "sc_dd_search_batch: row_stride smaller than num_channels");
+  }
+  if (count == 0) return SC_DD_OK;
+  DeviceGuard guard(dd->device);
+  return run_searches(dd, count, dev_inputs, row_strides, beams, coarse_channels, max_drift, min_drift,
+                      snr_threshold, out, capacity, num_hits, static_cast<cudaStream_t>(stream));
+}
+
+int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_stride, sc_dd_hit* hits,
+                               int num_hits, void* stream_ptr) {
   g_last_error.clear();
   if (!dd || !dev_input || (num_hits > 0 && !hits)) return fail(SC_DD_EINVAL, "sc_dd_add_incoherent_power: null argument");
   if (row_stride < dd->N) return fail(SC_DD_ESHAPE, "sc_dd_add_incoherent_power: row_stride smaller than num_channels");
@@ -360,6 +488,7 @@ int sc_dd_last_stats(const sc_dd* dd, sc_dd_stats* out) {
 
 int sc_dd_copy_channel_array(sc_dd* dd, int which, float* dst, void* stream_ptr) {
   if (!dd || !dst || (which != 0 && which != 1)) return fail(SC_DD_EINVAL, "sc_dd_copy_channel_array: bad argument");
+  if (dd->slots < 1) return fail(SC_DD_EINVAL, "sc_dd_copy_channel_array: no scratch");
   DeviceGuard guard(dd->device);
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   const float* src = which == 0 ? dd->top : dd->colsum;

@@ -10,7 +10,8 @@
 //   (dedoppler.cu:49-53); that is the first eligible path, in (drift block, offset)
 //   order, whose sum equals the final top sum.  The fused tree kernel keeps only the top
 //   value, so the few survivors recompute their paths here, bit-identically (pairwise
-//   tree order), and check the maximum against the stored top sum.
+//   tree order), one thread per (survivor, path); the host decodes the packed best and
+//   checks its sum against the stored top sum.
 // path_values_kernel: addIncoherentPower (dedoppler.cu:139-176): the path sum along a
 //   hit's path; the drift block is floor((float)drift_steps / (Tr-1)) in float, as there.
 #include "dd_common.cuh"
@@ -20,8 +21,12 @@ namespace scb {
 
 namespace {
 
-__global__ void window_kernel(const float* __restrict__ top, int N, int w, SearchHeader* hdr,
-                              Candidate* cands, int cap) {
+__global__ void window_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ top = sd.top;
+  const int N = sd.N, w = sd.window_size, cap = sd.cand_cap;
+  SearchHeader* hdr = sd.hdr;
+  Candidate* cands = sd.cands;
   const float thr = hdr->threshold;
   const int lane = threadIdx.x & 31;
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -55,54 +60,38 @@ __global__ void window_kernel(const float* __restrict__ top, int N, int w, Searc
     if (__any_sync(0xffffffffu, larger)) continue;
     if (lane == 0) {
       const int slot = atomicAdd(&hdr->num_candidates, 1);
-      if (slot < cap) cands[slot] = Candidate{(int)bidx, 0, best, 0};
+      if (slot < cap) cands[slot] = Candidate{(int)bidx, 0, best, 0, 0ull};
     }
   }
 }
 
-__global__ void resolve_kernel(const float* __restrict__ in, long long stride, int Tr, int N, int dmin,
-                               int dmax, SearchHeader* hdr, Candidate* cands, int cap) {
-  const int n = min(hdr->num_candidates, cap);
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  const int npaths = (dmax - dmin + 1) * Tr;
-  for (int i = gw; i < n; i += nw) {
+// One thread per (candidate, path): every eligible path of every surviving channel is
+// summed in tree order and folded into the candidate's packed best with atomicMax.
+__global__ void resolve_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ in = sd.input;
+  const long long stride = sd.row_stride;
+  const int Tr = sd.Tr, N = sd.N, dmin = sd.dmin, dmax = sd.dmax, cap = sd.cand_cap;
+  const SearchHeader* hdr = sd.hdr;
+  Candidate* cands = sd.cands;
+  const long long n = min(hdr->num_candidates, cap);
+  const long long npaths = (long long)(dmax - dmin + 1) * Tr;
+  const long long total = n * npaths;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long i = idx / npaths;
+    const int p = (int)(idx - i * npaths);
     const long long c = cands[i].index;
-    float best = 0.0f;  // the reference's top sums start at zero
-    int bp = -1;
-    for (int p = lane; p < npaths; p += 32) {
-      const int db = dmin + p / Tr;
-      const int off = p - (p / Tr) * Tr;
-      const long long e = (long long)(Tr - 1) * db;
-      if (c + e < 0 || c + e + off >= N) continue;
-      const float v = path_sum_pairwise(Tr, off, [&](int t, int pos) {
-        return __ldg(in + (long long)t * stride + c + (long long)db * t + pos);
-      });
-      if (v > best) {
-        best = v;
-        bp = p;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const float ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
-      if (op >= 0 && (bp < 0 || ov > best || (ov == best && op < bp))) {
-        best = ov;
-        bp = op;
-      }
-    }
-    if (lane == 0) {
-      if (bp >= 0) {
-        const int db = dmin + bp / Tr;
-        const int off = bp - (bp / Tr) * Tr;
-        cands[i].drift_steps = db * (Tr - 1) + off;
-        cands[i].flags = 1;
-        if (__float_as_int(best) != __float_as_int(cands[i].power)) atomicOr(&hdr->error, 1);
-      } else {
-        cands[i].drift_steps = 0;
-        cands[i].flags = 0;
-      }
+    const int db = dmin + p / Tr;
+    const int off = p - (p / Tr) * Tr;
+    const long long e = (long long)(Tr - 1) * db;
+    if (c + e < 0 || c + e + off >= N) continue;
+    const float v = path_sum_pairwise(Tr, off, [&](int t, int pos) {
+      return __ldg(in + (long long)t * stride + c + (long long)db * t + pos);
+    });
+    if (v > 0.0f) {  // the reference's top sums start at zero and update on strict >
+      const unsigned long long key = ((unsigned long long)float_key(v) << 32) | (unsigned long long)(~(uint32_t)p);
+      atomicMax(&cands[i].best, key);
     }
   }
 }
@@ -128,16 +117,21 @@ __global__ void path_values_kernel(const float* __restrict__ in, long long strid
 
 }  // namespace
 
-cudaError_t search_hits(const float* input, long long row_stride, int Tr, int N, const float* top,
-                        int window_size, int dmin, int dmax, SearchHeader* hdr, Candidate* cands,
-                        int cand_capacity, int num_sms, cudaStream_t stream) {
-  const long long nwin = ((long long)N + window_size - 1) / window_size;
-  long long wblocks = (nwin + 7) / 8;
-  if (wblocks > 8 * num_sms) wblocks = 8 * num_sms;
+cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t stream) {
+  if (b.count <= 0) return cudaSuccess;
+  long long nwin = 1;
+  for (int k = 0; k < b.count; ++k) {
+    const long long n = ((long long)b.s[k].N + b.s[k].window_size - 1) / b.s[k].window_size;
+    if (n > nwin) nwin = n;
+  }
+  long long wblocks = (nwin + 7) / 8;  // 8 warps per block, one window per warp
+  const long long wcap = (8ll * num_sms + b.count - 1) / b.count;
+  if (wblocks > wcap) wblocks = wcap;
   if (wblocks < 1) wblocks = 1;
-  window_kernel<<<(int)wblocks, 256, 0, stream>>>(top, N, window_size, hdr, cands, cand_capacity);
-  resolve_kernel<<<2 * num_sms, 256, 0, stream>>>(input, row_stride, Tr, N, dmin, dmax, hdr, cands,
-                                                   cand_capacity);
+  window_kernel<<<dim3((unsigned)wblocks, b.count), 256, 0, stream>>>(b);
+  int rblocks = (4 * num_sms + b.count - 1) / b.count;
+  if (rblocks < 4) rblocks = 4;
+  resolve_kernel<<<dim3(rblocks, b.count), 256, 0, stream>>>(b);
   return cudaGetLastError();
 }
 

@@ -6,38 +6,9 @@
 
 namespace scb {
 
-// One fused tree launch: jobs k = 0..n_jobs-1 read R rows starting at
-// rows + k*job_row_stride (row stride row_stride elements), sheared by d_first + k*d_step
-// channels per row.  Job k is drift
-// block db_first + k*db_step of the search and its in-block offset r is path offset
-// off_base + k*off_step + r; eligibility uses elig_T1 = rounded timesteps - 1.
-constexpr int kMaxSeg = 4;
-
-struct TreeParams {
-  const float* rows;
-  long long row_stride;
-  long long job_row_stride;  // 0: all jobs read the same rows; else job k reads rows + k*this
-  int N;
-  int d_first;
-  int d_step;                // job k is sheared by d_first + k*d_step channels per row
-  int n_jobs;
-  int db_first;
-  int db_step;
-  int off_base;
-  int off_step;
-  int elig_T1;
-  float* top;
-  // filled by the launcher
-  int jobs_per_chunk;
-  int n_chunks;
-  int n_tiles;
-};
-
-cudaError_t tree_max(const TreeParams& p, int R, int num_sms, cudaStream_t stream);
-
-}  // namespace scb
-
-namespace scb {
+constexpr int kMaxSeg = 4;       // staged windows per tree work item when jobs have their own rows
+constexpr int kMaxBatch = 64;    // searches per batched launch (descriptors travel as kernel parameters)
+constexpr int kVarChunks = 1024; // variance-emulation chunks per search, at most
 
 // Radix-select state for the three column-sum order statistics (first, mid, last).
 struct SelectState {
@@ -52,48 +23,122 @@ struct SelectState {
   long long n_lo, n_hi, n;
 };
 
-// Variance emulation scratch: per-chunk sums of the squared deviations and per-chunk
-// emulated contributions (kVarChunks entries each).
-constexpr int kVarChunks = 1024;
-
 struct MomentPartial {
   double s1, s2;  // s2 unused (kept for layout)
   unsigned long long lt_first, eq_first, lt_last, eq_last;
 };
 
-// A confirmed window maximum: channel, drift (filled by the resolve kernel), power.
+// A confirmed window maximum: channel and top sum, plus the best path found by the resolve
+// kernel, packed as (order key of the sum) << 32 | ~(path number) so that one 64-bit
+// atomicMax keeps the largest sum and, among equal sums, the first path.
 struct Candidate {
   int index;
-  int drift_steps;
+  int drift_steps;  // decoded from `best` on the host
   float power;
-  int flags;  // 1 = drift resolved
+  int flags;
+  unsigned long long best;
 };
 
 // Device-side result block of one search; the candidates follow it in memory.
 struct SearchHeader {
   int num_candidates;
-  int error;  // nonzero: a device-side consistency check failed
+  int error;
   int pad0, pad1;
   float median, std_dev, mean, threshold;
 };
 
-cudaError_t search_stats(const float* input, long long row_stride, int Tr, int N, float* colsum,
-                         SelectState* st, MomentPartial* partials, int n_partials, double* var_scratch,
-                         double snr_threshold, SearchHeader* hdr, int num_sms, cudaStream_t stream);
+// Everything the batched kernels need to know about one search.
+struct SearchDesc {
+  const float* input;
+  long long row_stride;
+  int Tr, N;
+  int dmin, dmax, window_size;
+  int first, mid, last;  // order-statistic ranks: ceil(0.05 N), N/2, floor(0.95 N)
+  double snr_threshold;
+  float* top;
+  float* colsum;
+  SelectState* sel;
+  MomentPartial* partials;  // at least as many as the statistics grid's x dimension
+  double* var;              // 2 * kVarChunks
+  SearchHeader* hdr;
+  Candidate* cands;
+  int cand_cap;
+  int pad;
+};
+
+struct SearchBatch {
+  int count;
+  int maxN;
+  SearchDesc s[kMaxBatch];
+};
+
+// One group of tree jobs (normally the drift blocks of one search): job k reads R rows
+// starting at rows + k*job_row_stride (row stride row_stride), sheared by
+// d_first + k*d_step channels per row; it is drift block db_first + k*db_step of its
+// search and its in-block offset r is path offset off_base + k*off_step + r; eligibility
+// uses elig_T1 = rounded timesteps - 1.  The launcher fills the scheduling fields.
+struct TreeGroup {
+  const float* rows;
+  long long row_stride;
+  long long job_row_stride;  // 0: all jobs read the same rows (one shared trapezoid)
+  int N;
+  int d_first;
+  int d_step;
+  int n_jobs;
+  int db_first;
+  int db_step;
+  int off_base;
+  int off_step;
+  int elig_T1;
+  float* top;
+  int jobs_per_chunk;
+  int n_chunks;
+  int n_tiles;
+  int item_begin;  // first work item of this group in the launch
+};
+
+struct TreeBatch {
+  int count;
+  int n_items;
+  TreeGroup g[kMaxBatch];
+};
+
+// Fused tree + per-channel top for the groups (all of R rows).  The launcher fills the
+// scheduling fields of `b` in place.
+cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream);
+
+// Column sums, order statistics, mean, standard deviation and threshold of each search.
+cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
 
 // Window de-duplication (dedoppler.cu:353-383) and drift recovery of the survivors.
-cudaError_t search_hits(const float* input, long long row_stride, int Tr, int N, const float* top,
-                        int window_size, int dmin, int dmax, SearchHeader* hdr, Candidate* cands,
-                        int cand_capacity, int num_sms, cudaStream_t stream);
+cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
 
 // Path sums along the given (index, drift_steps) paths: addIncoherentPower.
 cudaError_t path_values(const float* input, long long row_stride, int Tr, int N, const int* index,
                         const int* drift_steps, float* out, int n, cudaStream_t stream);
 
-// Multi-level tree for Tr > 16: level kernels write the partial planes of every
-// problem, then the last level runs the fused max kernel (see dd_levels.cu).
+// Multi-level tree for Tr > 16 (one search): level kernels write the partial planes of
+// every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).
 cudaError_t levels_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
                           cudaStream_t stream);
+
+// Decodes a resolved candidate: returns false if the recovered path sum does not equal the
+// stored top sum (a consistency failure).  Paths are numbered (db - dmin) * Tr + off.
+inline bool decode_candidate(const Candidate& c, int dmin, int Tr, int* drift_steps) {
+  if (c.best == 0ull) {  // no path sum above zero: the reference keeps no drift for it
+    *drift_steps = 0;
+    return true;
+  }
+  const uint32_t hi = (uint32_t)(c.best >> 32);
+  const uint32_t p = ~(uint32_t)(c.best & 0xffffffffull);
+  const uint32_t fbits = (hi & 0x80000000u) ? (hi & 0x7fffffffu) : ~hi;
+  uint32_t pbits;
+  __builtin_memcpy(&pbits, &c.power, 4);
+  const int db = dmin + (int)(p / (uint32_t)Tr);
+  const int off = (int)(p % (uint32_t)Tr);
+  *drift_steps = db * (Tr - 1) + off;
+  return fbits == pbits;
+}
 
 }  // namespace scb

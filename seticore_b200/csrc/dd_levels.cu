@@ -90,7 +90,11 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
       Tp /= M;
       dscale *= M;
     }
-    TreeParams tp{};
+    TreeBatch tb;
+    tb.count = 1;
+    tb.n_items = 0;
+    TreeGroup& tp = tb.g[0];
+    tp = TreeGroup{};
     tp.rows = src;
     tp.row_stride = N;
     tp.job_row_stride = 16ll * N;
@@ -104,7 +108,7 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     tp.off_step = 16;
     tp.elig_T1 = Tr - 1;
     tp.top = top;
-    cudaError_t err = tree_max(tp, 16, num_sms, stream);
+    cudaError_t err = tree_max_batch(tb, 16, num_sms, stream);
     if (err != cudaSuccess) return err;
   }
   return cudaGetLastError();

@@ -129,11 +129,40 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   if ((e = cudaMemsetAsync(top, 0, sizeof(float) * N, stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(hdr, 0, sizeof(scb::SearchHeader), stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: memset");
-  const int n_partials = std::min(kStaticPartials, 4 * num_sms);
-  if ((e = scb::search_stats(dev_input, row_stride, Tr, N, colsum, sel, partials, n_partials, var, snr_threshold,
-                             hdr, num_sms, stream)) != cudaSuccess)
+  // One-search batches; the descriptors travel as kernel parameters (no device copy).
+  // (About 15 KB of descriptors on the stack.)
+  scb::SearchBatch batch;
+  batch.count = 1;
+  batch.maxN = N;
+  scb::SearchDesc& sd = batch.s[0];
+  sd = scb::SearchDesc{};
+  sd.input = dev_input;
+  sd.row_stride = row_stride;
+  sd.Tr = Tr;
+  sd.N = N;
+  sd.dmin = dmin;
+  sd.dmax = dmax;
+  sd.window_size = window_size;
+  sd.first = (int)std::ceil(0.05 * N);
+  sd.mid = N / 2;
+  sd.last = (int)std::floor(0.95 * N);
+  sd.snr_threshold = snr_threshold;
+  sd.top = top;
+  sd.colsum = colsum;
+  sd.sel = sel;
+  sd.partials = partials;
+  sd.var = var;
+  sd.hdr = hdr;
+  sd.cands = cands;
+  sd.cand_cap = kStaticMaxCands;
+  if (kStaticPartials < 2 * num_sms) return fail(SC_DD_EINTERNAL, "sc_dd_search_static: too many SMs for the partials");
+  if ((e = scb::search_stats_batch(batch, num_sms, stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: statistics kernels");
-  scb::TreeParams tp{};
+  scb::TreeBatch tb;
+  tb.count = 1;
+  tb.n_items = 0;
+  scb::TreeGroup& tp = tb.g[0];
+  tp = scb::TreeGroup{};
   tp.rows = dev_input;
   tp.row_stride = row_stride;
   tp.job_row_stride = 0;
@@ -147,9 +176,9 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   tp.off_step = 0;
   tp.elig_T1 = Tr - 1;
   tp.top = top;
-  if ((e = scb::tree_max(tp, Tr, num_sms, stream)) != cudaSuccess) return cuda_fail(e, "sc_dd_search_static: tree kernel");
-  if ((e = scb::search_hits(dev_input, row_stride, Tr, N, top, window_size, dmin, dmax, hdr, cands, kStaticMaxCands,
-                            num_sms, stream)) != cudaSuccess)
+  if ((e = scb::tree_max_batch(tb, Tr, num_sms, stream)) != cudaSuccess)
+    return cuda_fail(e, "sc_dd_search_static: tree kernel");
+  if ((e = scb::search_hits_batch(batch, num_sms, stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: hit kernels");
 
   // Results through a stack buffer: the header, then the candidates in chunks.
@@ -157,7 +186,6 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   if ((e = cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: result copy");
-  if (h.error) return fail(SC_DD_EINTERNAL, "sc_dd_search_static: drift recovery did not reproduce a top sum");
   const int ncand = std::min(h.num_candidates, kStaticMaxCands);
   scb::Candidate chunk[kHostChunk];
   int n = 0;
@@ -169,13 +197,16 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
       return cuda_fail(e, "sc_dd_search_static: candidate copy");
     for (int i = 0; i < k; ++i) {
       const scb::Candidate& c = chunk[i];
-      const double drift_rate = c.drift_steps * res;  // dedoppler.cu:385-396
+      int drift_steps = 0;
+      if (!scb::decode_candidate(c, dmin, Tr, &drift_steps))
+        return fail(SC_DD_EINTERNAL, "sc_dd_search_static: drift recovery did not reproduce a top sum");
+      const double drift_rate = drift_steps * res;  // dedoppler.cu:385-396
       const float snr = (c.power - h.median) / h.std_dev;
       if (std::fabs(drift_rate) >= min_drift) {
         if (n < capacity) {
           sc_dd_hit& o = out[n];
           o.index = c.index;
-          o.drift_steps = c.drift_steps;
+          o.drift_steps = drift_steps;
           o.drift_rate = drift_rate;
           o.snr = snr;
           o.power = c.power;

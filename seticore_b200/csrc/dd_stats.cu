@@ -28,19 +28,23 @@ namespace scb {
 
 namespace {
 
-__global__ void colsum_kernel(const float* __restrict__ in, long long row_stride, int Tr, int N,
-                              float* __restrict__ colsum, SelectState* st, int r_first, int r_mid,
-                              int r_last) {
-  if (blockIdx.x == 0 && threadIdx.x < 3) {
-    const int r[3] = {r_first, r_mid, r_last};
-    st->prefix[threadIdx.x] = 0;
-    st->mask[threadIdx.x] = 0;
-    st->rank[threadIdx.x] = (uint32_t)r[threadIdx.x];
-    if (threadIdx.x == 0) st->ticket = 0;
-  }
+// Column sums of search blockIdx.y; block 0 also resets that search's select state.
+__global__ void colsum_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& d = b.s[blockIdx.y];
+  SelectState* st = d.sel;
   if (blockIdx.x == 0) {
+    if (threadIdx.x < 3) {
+      const int r = threadIdx.x == 0 ? d.first : (threadIdx.x == 1 ? d.mid : d.last);
+      st->prefix[threadIdx.x] = 0;
+      st->mask[threadIdx.x] = 0;
+      st->rank[threadIdx.x] = (uint32_t)r;
+      if (threadIdx.x == 0) st->ticket = 0;
+    }
     for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0;
   }
+  const float* in = d.input;
+  const long long row_stride = d.row_stride;
+  const int N = d.N, Tr = d.Tr;
   const bool vec = ((reinterpret_cast<uintptr_t>(in) & 15) == 0) && ((row_stride & 3) == 0) && ((N & 3) == 0);
   if (vec) {
     const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -53,31 +57,84 @@ __global__ void colsum_kernel(const float* __restrict__ in, long long row_stride
       acc.z += v.z;
       acc.w += v.w;
     }
-    reinterpret_cast<float4*>(colsum)[c4] = acc;
+    reinterpret_cast<float4*>(d.colsum)[c4] = acc;
   } else {
-    for (int c = blockIdx.x * blockDim.x * 4 + threadIdx.x; c < min(N, (blockIdx.x + 1) * blockDim.x * 4);
-         c += blockDim.x) {
+    const int c_end = min(N, (blockIdx.x + 1) * blockDim.x * 4);
+    for (int c = blockIdx.x * blockDim.x * 4 + threadIdx.x; c < c_end; c += blockDim.x) {
       float acc = 0.0f;
       for (int t = 0; t < Tr; ++t) acc += __ldg(in + (long long)t * row_stride + c);
-      colsum[c] = acc;
+      d.colsum[c] = acc;
     }
   }
 }
 
+// Adds 1 to hist[d] for every lane whose predicate holds, one atomic per distinct digit
+// in the warp (all channels often share the leading digits, so per-lane atomics on one bin
+// would serialise).
+__device__ __forceinline__ void warp_hist_add(unsigned* hist, uint32_t d, bool pred) {
+  const unsigned active = __ballot_sync(0xffffffffu, pred);
+  if (!pred) return;
+  const unsigned peers = __match_any_sync(active, d);
+  const int leader = __ffs(peers) - 1;
+  if ((int)(threadIdx.x & 31) == leader) atomicAdd(&hist[d], (unsigned)__popc(peers));
+}
+
+// Picks, for each target, the digit whose cumulative count passes its rank: 256 threads
+// scan the 256 bins in parallel.
+__device__ void select_digits(SelectState* st, int shift) {
+  __shared__ unsigned cnt[256];
+  __shared__ unsigned incl[256];
+  for (int j = 0; j < 3; ++j) {
+    const int d = threadIdx.x;
+    const uint32_t rank = st->rank[j];  // read before any thread can update it below
+    if (d < 256) cnt[d] = __ldcg(&st->hist[j][d]);
+    __syncthreads();
+    if (d < 256) {
+      unsigned v = cnt[d];
+      // inclusive scan over 256 bins (8 warps x 32) via shared memory doubling
+      incl[d] = v;
+    }
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+      unsigned add = 0;
+      if (d < 256 && d >= o) add = incl[d - o];
+      __syncthreads();
+      if (d < 256) incl[d] += add;
+      __syncthreads();
+    }
+    if (d < 256) {
+      const unsigned before = incl[d] - cnt[d];
+      if (rank >= before && rank < incl[d]) {
+        st->rank[j] = rank - before;
+        st->prefix[j] |= (uint32_t)d << shift;
+        st->mask[j] |= 255u << shift;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // One 8-bit radix-select pass for the three target ranks.
-__global__ void select_pass(const float* __restrict__ x, int N, SelectState* st, int shift) {
+__global__ void __launch_bounds__(256) select_pass(const __grid_constant__ SearchBatch b, int shift) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ x = sd.colsum;
+  const int N = sd.N;
+  SelectState* st = sd.sel;
   __shared__ unsigned hist[3][256];
   __shared__ bool last_block;
   for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t p0 = st->prefix[0], p1 = st->prefix[1], p2 = st->prefix[2];
   const uint32_t m0 = st->mask[0], m1 = st->mask[1], m2 = st->mask[2];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const uint32_t k = float_key(x[i]);
+  const int stride = gridDim.x * blockDim.x;
+  const int n_round = ((N + stride - 1) / stride) * stride;  // every lane runs the same trip count
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+    const bool in = i < N;
+    const uint32_t k = in ? float_key(x[i]) : 0u;
     const uint32_t d = (k >> shift) & 255u;
-    if ((k & m0) == p0) atomicAdd(&hist[0][d], 1u);
-    if ((k & m1) == p1) atomicAdd(&hist[1][d], 1u);
-    if ((k & m2) == p2) atomicAdd(&hist[2][d], 1u);
+    warp_hist_add(hist[0], d, in && (k & m0) == p0);
+    warp_hist_add(hist[1], d, in && (k & m1) == p1);
+    warp_hist_add(hist[2], d, in && (k & m2) == p2);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) {
@@ -91,31 +148,19 @@ __global__ void select_pass(const float* __restrict__ x, int N, SelectState* st,
   if (!last_block) return;
   __threadfence();
   // The last CTA: choose each target's digit, then clear the histogram for the next pass.
-  if (threadIdx.x < 3) {
-    const int j = threadIdx.x;
-    uint32_t rank = st->rank[j];
-    unsigned cum = 0;
-    int digit = 255;
-    for (int d = 0; d < 256; ++d) {
-      const unsigned h = __ldcg(&st->hist[j][d]);
-      if (rank < cum + h) {
-        digit = d;
-        break;
-      }
-      cum += h;
-    }
-    st->rank[j] = rank - cum;
-    st->prefix[j] |= (uint32_t)digit << shift;
-    st->mask[j] |= 255u << shift;
-  }
-  __syncthreads();
+  select_digits(st, shift);
   for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0;
   if (threadIdx.x == 0) st->ticket = 0;
 }
 
-__global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* st, int first,
-                               int last, double snr_threshold, MomentPartial* partials,
-                               SearchHeader* hdr) {
+__global__ void moments_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ x = sd.colsum;
+  const int N = sd.N;
+  SelectState* st = sd.sel;
+  const int first = sd.first, last = sd.last;
+  MomentPartial* partials = sd.partials;
+  SearchHeader* hdr = sd.hdr;
   __shared__ MomentPartial red[32];
   __shared__ bool last_block;
   const float v_first = key_float(st->prefix[0]);
@@ -157,16 +202,36 @@ __global__ void moments_kernel(const float* __restrict__ x, int N, SelectState* 
     last_block = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (!last_block || threadIdx.x != 0) return;
+  if (!last_block) return;
   __threadfence();
+  // Fixed-order reduction of the per-CTA partials: thread i folds partials i, i+256, ...,
+  // then the block reduces in warp/lane order (deterministic for a given grid).
   MomentPartial t = {0.0, 0.0, 0ull, 0ull, 0ull, 0ull};
-  for (int b = 0; b < (int)gridDim.x; ++b) {
-    const MomentPartial q = partials[b];
-    t.s1 += q.s1;
-    t.lt_first += q.lt_first;
-    t.eq_first += q.eq_first;
-    t.lt_last += q.lt_last;
-    t.eq_last += q.eq_last;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    t.s1 += __ldcg(&partials[b].s1);
+    t.lt_first += __ldcg(&partials[b].lt_first);
+    t.eq_first += __ldcg(&partials[b].eq_first);
+    t.lt_last += __ldcg(&partials[b].lt_last);
+    t.eq_last += __ldcg(&partials[b].eq_last);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    t.s1 += __shfl_down_sync(0xffffffffu, t.s1, o);
+    t.lt_first += __shfl_down_sync(0xffffffffu, t.lt_first, o);
+    t.eq_first += __shfl_down_sync(0xffffffffu, t.eq_first, o);
+    t.lt_last += __shfl_down_sync(0xffffffffu, t.lt_last, o);
+    t.eq_last += __shfl_down_sync(0xffffffffu, t.eq_last, o);
+  }
+  __syncthreads();
+  if (lane == 0) red[warp] = t;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  t = red[0];
+  for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+    t.s1 += red[w].s1;
+    t.lt_first += red[w].lt_first;
+    t.eq_first += red[w].eq_first;
+    t.lt_last += red[w].lt_last;
+    t.eq_last += red[w].eq_last;
   }
   st->ticket = 0;
   const long long n = (long long)last - first + 1;
@@ -213,8 +278,13 @@ __device__ __forceinline__ float var_term(float f, float m) {
 __device__ __forceinline__ bool var_inside(float f, float lo, float hi) { return f > lo && f < hi; }
 
 // Per-chunk exact sums of the terms of the channels strictly between the percentiles.
-__global__ void var_chunk_kernel(const float* __restrict__ x, int N, const SelectState* st, int chunk,
-                                 double* chunk_sum) {
+__global__ void var_chunk_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ x = sd.colsum;
+  const int N = sd.N;
+  const SelectState* st = sd.sel;
+  const int chunk = (N + gridDim.x - 1) / gridDim.x;
+  double* chunk_sum = sd.var;
   __shared__ double red[32];
   const float lo = key_float(st->prefix[0]), hi = key_float(st->prefix[2]);
   const float m = st->mean;
@@ -264,17 +334,31 @@ __device__ double block_exclusive_scan(double v, double* warp_tot, double* total
 
 // Emulates the float accumulation over every included term, in channel order, then the
 // boundary copies; the last CTA forms the standard deviation and the threshold.
-__global__ void var_emulate_kernel(const float* __restrict__ x, int N, SelectState* st, int chunk,
-                                   const double* chunk_sum, double* chunk_part, double snr_threshold,
-                                   SearchHeader* hdr) {
+__global__ void var_emulate_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ x = sd.colsum;
+  const int N = sd.N;
+  SelectState* st = sd.sel;
+  const int chunk = (N + gridDim.x - 1) / gridDim.x;
+  const double* chunk_sum = sd.var;
+  double* chunk_part = sd.var + kVarChunks;
+  const double snr_threshold = sd.snr_threshold;
+  SearchHeader* hdr = sd.hdr;
   __shared__ double warp_tot[32];
   __shared__ double tile_total;
   __shared__ double red[32];
   __shared__ bool last_block;
   const float lo = key_float(st->prefix[0]), hi = key_float(st->prefix[2]);
   const float m = st->mean;
+  // Exact sum of the preceding chunks, reduced in parallel.
+  double pre_part = 0.0;
+  for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) pre_part += chunk_sum[b];
+  for (int o = 16; o > 0; o >>= 1) pre_part += __shfl_down_sync(0xffffffffu, pre_part, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pre_part;
+  __syncthreads();
   double base = 0.0;
-  for (int b = 0; b < (int)blockIdx.x; ++b) base += chunk_sum[b];
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) base += red[w];
+  __syncthreads();
   const long long b0 = (long long)blockIdx.x * chunk;
   const long long b1 = min((long long)N, b0 + chunk);
   double contrib = 0.0;
@@ -303,12 +387,28 @@ __global__ void var_emulate_kernel(const float* __restrict__ x, int N, SelectSta
     last_block = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (!last_block || threadIdx.x != 0) return;
+  if (!last_block) return;
   __threadfence();
+  double pa = 0.0, pe = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    pa += __ldcg(chunk_part + b);
+    pe += __ldcg(chunk_sum + b);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    pa += __shfl_down_sync(0xffffffffu, pa, o);
+    pe += __shfl_down_sync(0xffffffffu, pe, o);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = pa;
+    warp_tot[threadIdx.x >> 5] = pe;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   double acc = 0.0, exact = 0.0;
-  for (int b = 0; b < (int)gridDim.x; ++b) {
-    acc += __ldcg(chunk_part + b);
-    exact += __ldcg(chunk_sum + b);
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    acc += red[w];
+    exact += warp_tot[w];
   }
   // The percentile values themselves (ties at the boundaries), added after the rest.
   const double tlo = (double)var_term(lo, m), thi = (double)var_term(hi, m);
@@ -329,28 +429,24 @@ __global__ void var_emulate_kernel(const float* __restrict__ x, int N, SelectSta
 
 }  // namespace
 
-cudaError_t search_stats(const float* input, long long row_stride, int Tr, int N, float* colsum,
-                         SelectState* st, MomentPartial* partials, int n_partials, double* var_scratch,
-                         double snr_threshold, SearchHeader* hdr, int num_sms, cudaStream_t stream) {
-  const int first = (int)ceil(0.05 * N);
-  const int last = (int)floor(0.95 * N);
-  const int mid = N / 2;
-  const int cblocks = (N + 4 * 256 - 1) / (4 * 256);
-  colsum_kernel<<<cblocks, 256, 0, stream>>>(input, row_stride, Tr, N, colsum, st, first, mid, last);
-  int sblocks = 2 * num_sms;
-  const int max_needed = (N + 255) / 256;
-  if (sblocks > max_needed) sblocks = max_needed;
-  for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<sblocks, 256, 0, stream>>>(colsum, N, st, shift);
-  int mblocks = sblocks < n_partials ? sblocks : n_partials;
-  moments_kernel<<<mblocks, 256, 0, stream>>>(colsum, N, st, first, last, snr_threshold, partials, hdr);
-  int vchunks = 2 * num_sms;
+cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream) {
+  if (b.count <= 0) return cudaSuccess;
+  const int maxN = b.maxN;
+  dim3 cgrid((maxN + 4 * 256 - 1) / (4 * 256), b.count);
+  colsum_kernel<<<cgrid, 256, 0, stream>>>(b);
+  // About four CTAs per SM over the whole batch, at least 8 per search.
+  int sblocks = (4 * num_sms + b.count - 1) / b.count;
+  if (sblocks < 8) sblocks = 8;
+  if (sblocks > 2 * num_sms) sblocks = 2 * num_sms;
+  if (sblocks > (maxN + 255) / 256) sblocks = (maxN + 255) / 256;
+  dim3 sgrid(sblocks, b.count);
+  for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<sgrid, 256, 0, stream>>>(b, shift);
+  moments_kernel<<<sgrid, 256, 0, stream>>>(b);
+  int vchunks = sblocks;
   if (vchunks > kVarChunks) vchunks = kVarChunks;
-  if (vchunks > (N + 255) / 256) vchunks = (N + 255) / 256;
-  const int chunk = (N + vchunks - 1) / vchunks;
-  vchunks = (N + chunk - 1) / chunk;
-  var_chunk_kernel<<<vchunks, 256, 0, stream>>>(colsum, N, st, chunk, var_scratch);
-  var_emulate_kernel<<<vchunks, 256, 0, stream>>>(colsum, N, st, chunk, var_scratch, var_scratch + kVarChunks,
-                                                  snr_threshold, hdr);
+  dim3 vgrid(vchunks, b.count);
+  var_chunk_kernel<<<vgrid, 256, 0, stream>>>(b);
+  var_emulate_kernel<<<vgrid, 256, 0, stream>>>(b);
   return cudaGetLastError();
 }
 

@@ -14,8 +14,12 @@ reads each input value from shared memory once.  The in-block offsets [lo, hi) o
 root are a parameter: splitting the offsets over two warps halves the registers a lane
 needs without duplicating any add (the two halves share no tree node above the leaves).
 
-The emitted function is straight-line code; the CUDA compiler allocates registers for
-the windows.  Each value is emitted in the order of the first channel that consumes it.
+The emitted function is a loop over the strip, U channels per iteration: a prologue
+fills every node's window for the first channel, the loop body is straight-line code for
+U channels, and the values a later iteration still needs are carried in registers across
+the back edge.  Looping (rather than unrolling the whole strip) keeps the code of one
+offset half small enough for the instruction cache.  Each iteration folds its U outputs
+per channel into the warp's row of per-channel maxima in shared memory.
 """
 import os
 import sys
@@ -36,62 +40,124 @@ def consumption(R, lo, hi):
     return pos
 
 
-def gen_strip(R, lo, hi, S):
-    pos = consumption(R, lo, hi)
-    stmts = []  # (first_step, level, text)
-
-    def name(L, b, o, p):
-        return f"v{L}_{b}_{o}_{p}".replace("-", "m")
-
-    for (L, b, o), P in pos.items():
-        needed = sorted({s + p for s in range(S) for p in P})
-        for q in needed:
-            first = q - max(P)
-            if L == 1:
-                text = f"const float {name(L, b, o, q)} = row[{b}][{q}];"
-            else:
-                sh = (o + 1) // 2
-                text = (f"const float {name(L, b, o, q)} = "
-                        f"{name(L // 2, 2 * b, o // 2, q)} + {name(L // 2, 2 * b + 1, o // 2, q + sh)};")
-            stmts.append((first, L, text))
-    # fold the root outputs of each step into the running maximum, three at a time
-    for s in range(S):
-        outs = [name(R, 0, o, s) for o in range(lo, hi)]
-        acc = f"m[{s}]"
-        i = 0
-        while i < len(outs):
-            if i + 1 < len(outs):
-                stmts.append((s, R + 1, f"{acc} = fmax3({acc}, {outs[i]}, {outs[i + 1]});"))
-                i += 2
-            else:
-                stmts.append((s, R + 1, f"{acc} = fmaxf({acc}, {outs[i]});"))
-                i += 1
-    stmts.sort(key=lambda x: (x[0], x[1]))
-    body = "\n".join("  " + t for _, _, t in stmts)
-    return (f"template <>\n__device__ __forceinline__ void taylor_strip_max<{R}, {lo}, {hi}, {S}>(\n"
-            f"    const float* const (&row)[{R}], float (&m)[{S}]) {{\n{body}\n}}\n")
-
-
 def lead(R, lo, hi):
     """Largest channel offset a strip reads beyond its last output channel."""
     pos = consumption(R, lo, hi)
     return max(max(P) for (L, b, o), P in pos.items() if L == 1)
 
 
-# (R, parts, S) combinations compiled into the library.
-CONFIGS = [(2, 1, 33), (4, 1, 33), (8, 1, 33), (16, 2, 33)]
+def gen_strip_loop(R, lo, hi, U, ITERS):
+    """Looped form: a prologue fills every node's window for step 0, then ITERS iterations
+    of a U-step body; values still needed after an iteration are carried into the next
+    (the loop-carried registers), and each iteration folds its U per-channel maxima into the
+    warp's row of shared memory (mrow[0..U*ITERS))."""
+    pos = consumption(R, lo, hi)
+    nodes = {k: (min(P), max(P)) for k, P in pos.items() if k[0] != R}  # (mn, lead)
+    roots = [(R, 0, o) for o in range(lo, hi)]
+
+    def nm(L, b, o):
+        return f"{L}_{b}_{o}"
+
+    def val(L, b, o, j):
+        return f"v{nm(L, b, o)}_{j}".replace("-", "m")
+
+    def st(L, b, o, k):
+        return f"s{nm(L, b, o)}[{k}]"
+
+    order = sorted(nodes.keys(), key=lambda k: k[0])  # leaves first, then bottom-up
+    lines = []
+    # state arrays
+    for (L, b, o) in order:
+        mn, ld = nodes[(L, b, o)]
+        if ld - mn >= 1:
+            lines.append(f"  float s{nm(L, b, o)}[{ld - mn}];")
+    # prologue: positions [mn, lead-1] of every node (bottom-up)
+    def compute(L, b, o, j, src_pos_name):
+        if L == 1:
+            return f"row[{b}][{j}]"
+        sh = (o + 1) // 2
+        return f"{src_pos_name(L // 2, 2 * b, o // 2, j)} + {src_pos_name(L // 2, 2 * b + 1, o // 2, j + sh)}"
+
+    def prologue_name(L, b, o, j):
+        mn, ld = nodes[(L, b, o)]
+        return st(L, b, o, j - mn)
+
+    # Prologue in order of position then level, so children exist before parents.
+    pro = []
+    for (L, b, o) in order:
+        mn, ld = nodes[(L, b, o)]
+        for j in range(mn, ld):
+            pro.append((j - ld, L, f"  {prologue_name(L, b, o, j)} = {compute(L, b, o, j, prologue_name)};"))
+    pro.sort(key=lambda x: (x[0], x[1]))
+    lines += [t for _, _, t in pro]
+    lines.append(f"#pragma unroll 1")
+    lines.append(f"  for (int it = 0; it < {ITERS}; ++it) {{")
+    lines.append(f"    const int base = it * {U};")
+
+    # body: value names for positions j in [mn, U-1+lead] relative to iteration start
+    def body_name(L, b, o, j):
+        mn, ld = nodes[(L, b, o)]
+        if j < ld:
+            return st(L, b, o, j - mn)
+        return val(L, b, o, j)
+
+    body = []
+    for (L, b, o) in order:
+        mn, ld = nodes[(L, b, o)]
+        for j in range(ld, U + ld):
+            if L == 1:
+                expr = f"row[{b}][base + {j}]"
+            else:
+                expr = compute(L, b, o, j, body_name)
+            body.append((j - ld, L, f"    const float {val(L, b, o, j)} = {expr};"))
+    for s in range(U):
+        outs = []
+        for (_, _, o) in roots:
+            sh = (o + 1) // 2
+            outs.append(f"{body_name(R // 2, 0, o // 2, s)} + {body_name(R // 2, 1, o // 2, s + sh)}")
+        body.append((s, R, f"    float m{s} = mrow[base + {s}];"))
+        for i, e in enumerate(outs):
+            body.append((s, R, f"    const float o{s}_{i} = {e};"))
+        acc = f"m{s}"
+        i = 0
+        while i < len(outs):
+            if i + 1 < len(outs):
+                body.append((s, R + 1, f"    {acc} = fmax3({acc}, o{s}_{i}, o{s}_{i + 1});"))
+                i += 2
+            else:
+                body.append((s, R + 1, f"    {acc} = fmaxf({acc}, o{s}_{i});"))
+                i += 1
+        body.append((s, R + 2, f"    mrow[base + {s}] = {acc};"))
+    body.sort(key=lambda x: (x[0], x[1]))
+    lines += [t for _, _, t in body]
+    # carry: new state k holds position U + mn + k
+    carry = []
+    for (L, b, o) in order:
+        mn, ld = nodes[(L, b, o)]
+        for k in range(ld - mn):
+            carry.append(f"    {st(L, b, o, k)} = {body_name(L, b, o, U + mn + k)};")
+    lines += carry
+    lines.append("  }")
+    body_text = "\n".join(lines)
+    return (f"template <>\n__device__ __forceinline__ void taylor_strip_loop<{R}, {lo}, {hi}, {U}, {ITERS}>(\n"
+            f"    const float* const (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
+
+
+# (R, offset parts, U steps per iteration, iterations) compiled into the library; a strip is
+# S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks).
+LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3)]
 
 
 def main(out_path):
     parts = [
         "// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n",
-        "template <int R, int LO, int HI, int S>\n"
-        "__device__ __forceinline__ void taylor_strip_max(const float* const (&row)[R], float (&m)[S]);\n",
+        "template <int R, int LO, int HI, int U, int ITERS>\n"
+        "__device__ __forceinline__ void taylor_strip_loop(const float* const (&row)[R], float* __restrict__ mrow);\n",
     ]
-    for R, nparts, S in CONFIGS:
+    for R, nparts, U, IT in LOOP_CONFIGS:
         step = R // nparts
         for k in range(nparts):
-            parts.append(gen_strip(R, k * step, (k + 1) * step, S))
+            parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT))
     text = "\n".join(parts)
     if os.path.exists(out_path) and open(out_path).read() == text:
         return

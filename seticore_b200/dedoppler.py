@@ -217,6 +217,44 @@ class Dedopplerer:
             check(rc)
             return list(buf[: n.value])
 
+    def search_batch_raw(self, inputs, beams, coarse_channels, max_drift: float, min_drift: float,
+                         snr_threshold: float, stream=None, capacity: int = 1 << 16):
+        """Many searches of this engine's shape in one call (sc_dd_search_batch).  Returns one
+        list of ScDdHit per input."""
+        ts = [_device_input(x, self.rounded_num_timesteps, self.num_channels) for x in inputs]
+        n = len(ts)
+        if n == 0:
+            return []
+        ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in ts])
+        strides = (ctypes.c_longlong * n)(*[t.stride(0) for t in ts])
+        b = (ctypes.c_int * n)(*beams)
+        c = (ctypes.c_int * n)(*coarse_channels)
+        counts = (ctypes.c_int * n)()
+        cap = capacity
+        while True:
+            buf = (_capi.ScDdHit * max(cap, 1))()
+            rc = lib().sc_dd_search_batch(self._h, n, ptrs, strides, b, c, max_drift, min_drift, snr_threshold,
+                                          buf, cap, counts, _stream_handle(stream))
+            if rc == _capi.SC_DD_ETRUNC:
+                cap = sum(counts)
+                continue
+            check(rc)
+            out, k = [], 0
+            for cnt in counts:
+                out.append(list(buf[k:k + cnt]))
+                k += cnt
+            return out
+
+    def search_batch(self, inputs, metadata: Optional[FilterbankMetadata], beams, coarse_channels,
+                     max_drift: float, min_drift: float, snr_threshold: float, stream=None) -> list:
+        """Batched Dedopplerer::search: one list of DedopplerHit per input."""
+        meta = metadata or FilterbankMetadata(foff=self.foff, tsamp=self.tsamp,
+                                              coarse_channel_size=self.num_channels)
+        res = self.search_batch_raw(inputs, beams, coarse_channels, max_drift, min_drift, snr_threshold, stream)
+        return [[DedopplerHit.make(meta, h.index, h.drift_steps, h.drift_rate, h.snr, b, c, self.num_timesteps,
+                                   h.power) for h in hits]
+                for hits, b, c in zip(res, beams, coarse_channels)]
+
     def search(self, input, metadata: Optional[FilterbankMetadata], beam: int, coarse_channel: int,
                max_drift: float, min_drift: float, snr_threshold: float,
                output: Optional[list] = None, stream=None) -> list:

@@ -215,3 +215,23 @@ def test_cpp_dropin_known_answer(torch_cuda):
         pytest.fail("C++ test program not built (python -m seticore_b200.build)")
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_batch_equals_single_searches(torch_cuda):
+    """sc_dd_search_batch over 70 inputs (two launches of up to 64) equals 70 single searches."""
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_torch
+    torch = torch_cuda
+    N = 1 << 15
+    specs = [SearchSpec(16, N, seed=500 + i, n_tones=4, n_spikes=1, snr_threshold=8.0) for i in range(70)]
+    data = torch.empty((70, 16, N), dtype=torch.float32, device="cuda")
+    for i, s in enumerate(specs):
+        make_filterbank_torch(s, out=data[i])
+    dd = Dedopplerer(16, N, specs[0].foff_mhz, specs[0].tsamp)
+    single = [dd.search_raw(data[i], -1, i, 4.0, 0.0, 8.0) for i in range(70)]
+    batch = dd.search_batch_raw([data[i] for i in range(70)], [-1] * 70, list(range(70)), 4.0, 0.0, 8.0)
+    assert len(batch) == 70
+    for a, b in zip(single, batch):
+        assert [(h.index, h.drift_steps, h.power, h.snr, h.coarse_channel) for h in a] == \
+               [(h.index, h.drift_steps, h.power, h.snr, h.coarse_channel) for h in b]
+    assert sum(len(x) for x in batch) > 70
