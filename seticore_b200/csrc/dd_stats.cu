@@ -68,15 +68,21 @@ __global__ void colsum_kernel(const __grid_constant__ SearchBatch b) {
   }
 }
 
-// Adds 1 to hist[d] for every lane whose predicate holds, one atomic per distinct digit
-// in the warp (all channels often share the leading digits, so per-lane atomics on one bin
-// would serialise).
+// Adds 1 to hist[d] for every lane whose predicate holds.  When every counted lane has
+// the same digit (common for the leading digits: neighbouring channels have similar sums)
+// one atomic adds them all; otherwise each lane adds to its warp's private histogram, so
+// only lanes of one warp with equal digits contend.
 __device__ __forceinline__ void warp_hist_add(unsigned* hist, uint32_t d, bool pred) {
   const unsigned active = __ballot_sync(0xffffffffu, pred);
-  if (!pred) return;
-  const unsigned peers = __match_any_sync(active, d);
-  const int leader = __ffs(peers) - 1;
-  if ((int)(threadIdx.x & 31) == leader) atomicAdd(&hist[d], (unsigned)__popc(peers));
+  if (active == 0u) return;
+  const int first = __ffs(active) - 1;
+  const uint32_t d0 = __shfl_sync(0xffffffffu, d, first);
+  const bool same = __all_sync(0xffffffffu, !pred || d == d0);
+  if (same) {
+    if ((int)(threadIdx.x & 31) == first) atomicAdd(&hist[d0], (unsigned)__popc(active));
+  } else if (pred) {
+    atomicAdd(&hist[d], 1u);
+  }
 }
 
 // Picks, for each target, the digit whose cumulative count passes its rank: 256 threads
@@ -120,10 +126,11 @@ __global__ void __launch_bounds__(256) select_pass(const __grid_constant__ Searc
   const float* __restrict__ x = sd.colsum;
   const int N = sd.N;
   SelectState* st = sd.sel;
-  __shared__ unsigned hist[3][256];
+  __shared__ unsigned whist[8][3][256];  // one histogram per warp
   __shared__ bool last_block;
-  for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&hist[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < 8 * 3 * 256; i += blockDim.x) (&whist[0][0][0])[i] = 0;
   __syncthreads();
+  unsigned (*hist)[256] = whist[threadIdx.x >> 5];
   const uint32_t p0 = st->prefix[0], p1 = st->prefix[1], p2 = st->prefix[2];
   const uint32_t m0 = st->mask[0], m1 = st->mask[1], m2 = st->mask[2];
   const int stride = gridDim.x * blockDim.x;
@@ -137,8 +144,10 @@ __global__ void __launch_bounds__(256) select_pass(const __grid_constant__ Searc
     warp_hist_add(hist[2], d, in && (k & m2) == p2);
   }
   __syncthreads();
+  const int nw = blockDim.x >> 5;
   for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) {
-    const unsigned v = (&hist[0][0])[i];
+    unsigned v = 0;
+    for (int w = 0; w < nw; ++w) v += (&whist[w][0][0])[i];
     if (v) atomicAdd(&st->hist[0][0] + i, v);
   }
   __threadfence();

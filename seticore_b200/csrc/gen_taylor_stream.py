@@ -18,8 +18,9 @@ The emitted function is a loop over the strip, U channels per iteration: a prolo
 fills every node's window for the first channel, the loop body is straight-line code for
 U channels, and the values a later iteration still needs are carried in registers across
 the back edge.  Looping (rather than unrolling the whole strip) keeps the code of one
-offset half small enough for the instruction cache.  Each iteration folds its U outputs
-per channel into the warp's row of per-channel maxima in shared memory.
+offset half small enough for the instruction cache.  Each channel's outputs are folded into
+a running maximum (starting at 0, so NaN and negative sums never count) that fold_max()
+merges into the CTA's per-channel maxima in shared memory.
 """
 import os
 import sys
@@ -115,7 +116,7 @@ def gen_strip_loop(R, lo, hi, U, ITERS):
         for (_, _, o) in roots:
             sh = (o + 1) // 2
             outs.append(f"{body_name(R // 2, 0, o // 2, s)} + {body_name(R // 2, 1, o // 2, s + sh)}")
-        body.append((s, R, f"    float m{s} = mrow[base + {s}];"))
+        body.append((s, R, f"    float m{s} = 0.0f;"))
         for i, e in enumerate(outs):
             body.append((s, R, f"    const float o{s}_{i} = {e};"))
         acc = f"m{s}"
@@ -127,7 +128,7 @@ def gen_strip_loop(R, lo, hi, U, ITERS):
             else:
                 body.append((s, R + 1, f"    {acc} = fmaxf({acc}, o{s}_{i});"))
                 i += 1
-        body.append((s, R + 2, f"    mrow[base + {s}] = {acc};"))
+        body.append((s, R + 2, f"    fold_max(mrow + base + {s}, {acc});"))
     body.sort(key=lambda x: (x[0], x[1]))
     lines += [t for _, _, t in body]
     # carry: new state k holds position U + mn + k
