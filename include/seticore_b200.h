@@ -60,7 +60,20 @@ typedef struct sc_dd_stats {
   int num_candidates; /* window maxima above threshold, before the min_drift filter */
   float tree_ms;      /* device time of the Taylor-tree kernel(s), CUDA events on the stream */
   float search_ms;    /* device time of the whole search, first memset to last kernel */
+  int precision;          /* SC_DD_PRECISION_* of the search */
+  int recomputed_tiles;   /* precision form: tiles recomputed exactly in FP32 */
+  int total_tiles;        /* tiles of W channels in a coarse channel */
+  int pad;
+  double norm_mean;       /* precision form: FP64 mean of the power, used to normalise */
+  double norm_std;        /* precision form: FP64 standard deviation, used to normalise */
 } sc_dd_stats;
+
+/* Storage of the spectra the tree reads.  FP32: the input as given (the reference's
+ * form).  BF16 / FP16: each search first normalises its input per coarse channel,
+ * (x - mean) / std with FP64 mean and std, into a 16-bit copy; the tree accumulates in
+ * FP32 over that copy, every tile holding a channel within 0.9 x the threshold is then
+ * recomputed in FP32 from the original power, and the hit list equals the FP32 form's. */
+enum { SC_DD_PRECISION_FP32 = 0, SC_DD_PRECISION_BF16 = 1, SC_DD_PRECISION_FP16 = 2 };
 
 typedef struct sc_dd sc_dd;
 
@@ -110,12 +123,17 @@ int sc_dd_search_batch(sc_dd* dd, int count, const float* const* dev_inputs,
 int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_stride,
                                sc_dd_hit* hits, int num_hits, void* stream);
 
+/* Selects the storage form of later searches (SC_DD_PRECISION_*).  The 16-bit forms
+ * support up to 16 rounded timesteps; they allocate their scratch on first use. */
+int sc_dd_set_precision(sc_dd* dd, int precision);
+
 /* Statistics of the first search of the engine's last completed call; tree_ms and
  * search_ms time its first batch of up to 64 searches. */
 int sc_dd_last_stats(const sc_dd* dd, sc_dd_stats* out);
 
-/* Copies an internal per-channel array of the last search into dst (any memory
- * cudaMemcpy can reach): which = 0 top path sums, 1 column sums.  N floats. */
+/* Copies an internal per-channel array of the first search of the last call into dst
+ * (any memory cudaMemcpy can reach): which = 0 top path sums, 1 column sums, 2 the 16-bit
+ * form's approximate tops in normalised units.  N floats. */
 int sc_dd_copy_channel_array(sc_dd* dd, int which, float* dst, void* stream);
 
 /* Message of the calling thread's last failed call ("" if none). */

@@ -16,13 +16,17 @@ SC_DD_ETRUNC = 4
 SC_DD_EINTERNAL = 5
 SC_DD_ESHAPE = 6
 SC_DD_ELIMIT = 7
+SC_DD_PRECISION_FP32 = 0
+SC_DD_PRECISION_BF16 = 1
+SC_DD_PRECISION_FP16 = 2
 SC_DD_STATIC_MAX_CHANNELS = 1048576
 NO_BEAM = -1
 
 # Every symbol the header declares; tests check the library exports all of them.
 EXPORTED = [
     "sc_dd_create", "sc_dd_destroy", "sc_dd_memory_usage", "sc_dd_rounded_timesteps",
-    "sc_dd_search", "sc_dd_search_batch", "sc_dd_add_incoherent_power", "sc_dd_last_stats",
+    "sc_dd_search", "sc_dd_search_batch", "sc_dd_add_incoherent_power", "sc_dd_set_precision",
+    "sc_dd_last_stats",
     "sc_dd_copy_channel_array", "sc_dd_last_error", "sc_dd_version", "sc_dd_search_static",
 ]
 
@@ -53,6 +57,12 @@ class ScDdStats(ctypes.Structure):
         ("num_candidates", ctypes.c_int),
         ("tree_ms", ctypes.c_float),
         ("search_ms", ctypes.c_float),
+        ("precision", ctypes.c_int),
+        ("recomputed_tiles", ctypes.c_int),
+        ("total_tiles", ctypes.c_int),
+        ("pad", ctypes.c_int),
+        ("norm_mean", ctypes.c_double),
+        ("norm_std", ctypes.c_double),
     ]
 
 
@@ -85,6 +95,7 @@ def lib():
                                          ctypes.POINTER(i), vp]
         L.sc_dd_add_incoherent_power.argtypes = [vp, vp, ll, ctypes.POINTER(ScDdHit), i, vp]
         L.sc_dd_last_stats.argtypes = [vp, ctypes.POINTER(ScDdStats)]
+        L.sc_dd_set_precision.argtypes = [vp, i]
         L.sc_dd_search_static.argtypes = [vp, ll, i, i, d, d, i, i, d, d, d, ctypes.POINTER(ScDdHit), i,
                                           ctypes.POINTER(i), vp]
         L.sc_dd_copy_channel_array.argtypes = [vp, i, vp, vp]

@@ -99,6 +99,18 @@ struct sc_dd {
   int* inc_steps = nullptr;
   float* inc_vals = nullptr;
   int inc_cap = 0;
+  // Precision form (16-bit normalised storage), per slot.
+  int precision = SC_DD_PRECISION_FP32;
+  int prec_slots = 0;
+  void* norm16 = nullptr;        // [slot][Tr][N] 16-bit
+  float* top16 = nullptr;        // [slot][N]
+  int* tiles = nullptr;          // [slot][max_tiles]
+  int* tile_counts = nullptr;    // [slot]
+  double* norm_moments = nullptr;  // [slot][2 * kVarChunks + 2]
+  unsigned* norm_tickets = nullptr;  // [slot]
+  int* host_tile_counts = nullptr;   // pinned [slot]
+  double* host_norm = nullptr;       // pinned [2]: mean, std of search 0
+  int max_tiles = 0;
   size_t device_bytes = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, tree start/end, call end
   sc_dd_stats last{};
@@ -142,8 +154,49 @@ void free_slots(sc_dd* d) {
   d->slots = 0;
 }
 
+void free_prec(sc_dd* d) {
+  const size_t S = d->prec_slots, N = d->N;
+  dfree(d, &d->norm16, 2 * N * d->Tr * S);
+  dfree(d, &d->top16, sizeof(float) * N * S);
+  dfree(d, &d->tiles, sizeof(int) * d->max_tiles * S);
+  dfree(d, &d->tile_counts, sizeof(int) * S);
+  dfree(d, &d->norm_moments, sizeof(double) * (2 * scb::kVarChunks + 2) * S);
+  dfree(d, &d->norm_tickets, sizeof(unsigned) * S);
+  if (d->host_tile_counts) cudaFreeHost(d->host_tile_counts);
+  if (d->host_norm) cudaFreeHost(d->host_norm);
+  d->host_tile_counts = nullptr;
+  d->host_norm = nullptr;
+  d->prec_slots = 0;
+}
+
+int ensure_prec(sc_dd* d, int slots) {
+  if (slots <= d->prec_slots) return SC_DD_OK;
+  cudaDeviceSynchronize();
+  free_prec(d);
+  const size_t S = slots, N = d->N;
+  d->max_tiles = (d->N + scb::tree_tile_width() - 1) / scb::tree_tile_width();
+  cudaError_t e;
+  if ((e = dalloc(d, &d->norm16, 2 * N * d->Tr * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->top16, sizeof(float) * N * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->tiles, sizeof(int) * d->max_tiles * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->tile_counts, sizeof(int) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->norm_moments, sizeof(double) * (2 * scb::kVarChunks + 2) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->norm_tickets, sizeof(unsigned) * S)) != cudaSuccess ||
+      (e = cudaMallocHost(&d->host_tile_counts, sizeof(int) * S)) != cudaSuccess ||
+      (e = cudaMallocHost(&d->host_norm, sizeof(double) * 2)) != cudaSuccess) {
+    d->prec_slots = slots;
+    free_prec(d);
+    return fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA,
+                std::string("precision scratch allocation failed: ") + cudaGetErrorString(e));
+  }
+  d->prec_slots = slots;
+  if ((e = cudaMemset(d->norm_tickets, 0, sizeof(unsigned) * S)) != cudaSuccess) return cuda_fail(e, "memset");
+  return SC_DD_OK;
+}
+
 void free_all(sc_dd* d) {
   free_slots(d);
+  free_prec(d);
   dfree(d, &d->scratch_a, sizeof(float) * (size_t)d->N * d->Tr);
   dfree(d, &d->scratch_b, sizeof(float) * (size_t)d->N * d->Tr);
   dfree(d, &d->inc_index, sizeof(int) * d->inc_cap);
@@ -235,9 +288,69 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
   if ((e = cudaMemsetAsync(dd->top, 0, sizeof(float) * dd->N * (size_t)n, stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(dd->hdrs, 0, sizeof(scb::SearchHeader) * n, stream)) != cudaSuccess)
     return cuda_fail(e, "memset");
+  const bool prec = dd->precision != SC_DD_PRECISION_FP32;
+  const int elem16 = dd->precision == SC_DD_PRECISION_BF16 ? scb::kElemBF16 : scb::kElemF16;
+  scb::PrecisionBatch pb;
+  if (prec) {
+    pb.count = n;
+    pb.maxN = dd->N;
+    pb.elem = elem16;
+    for (int k = 0; k < n; ++k) {
+      scb::PrecisionDesc& q = pb.s[k];
+      q.input = inputs[k];
+      q.row_stride = strides[k];
+      q.T = dd->T;
+      q.Tr = dd->Tr;
+      q.N = dd->N;
+      q.norm = static_cast<char*>(dd->norm16) + (size_t)2 * dd->N * dd->Tr * k;
+      q.moments = dd->norm_moments + (size_t)(2 * scb::kVarChunks + 2) * k;
+      q.ticket = dd->norm_tickets + k;
+      q.top16 = dd->top16 + (size_t)dd->N * k;
+      q.hdr = b.s[k].hdr;
+      q.snr_threshold = snr_threshold;
+      q.tile_list = dd->tiles + (size_t)dd->max_tiles * k;
+      q.tile_count = dd->tile_counts + k;
+    }
+    if ((e = cudaMemsetAsync(dd->top16, 0, sizeof(float) * dd->N * (size_t)n, stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(dd->tile_counts, 0, sizeof(int) * n, stream)) != cudaSuccess)
+      return cuda_fail(e, "memset");
+    if ((e = scb::normalize_batch(pb, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "normalisation kernels");
+  }
   if ((e = scb::search_stats_batch(b, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "statistics kernels");
   if (first_batch) cudaEventRecord(dd->ev[1], stream);
-  if (dd->Tr <= 16) {
+  if (prec) {
+    // Approximate tops over the 16-bit copy, flags, then exact FP32 tops of flagged tiles.
+    scb::TreeBatch tb;
+    tb.count = n;
+    tb.n_items = 0;
+    for (int k = 0; k < n; ++k) {
+      scb::TreeGroup& g = tb.g[k];
+      g = scb::TreeGroup{};
+      g.rows = pb.s[k].norm;
+      g.row_stride = dd->N;
+      g.N = dd->N;
+      g.d_first = p.dmin;
+      g.d_step = 1;
+      g.n_jobs = p.dmax - p.dmin + 1;
+      g.db_first = p.dmin;
+      g.db_step = 1;
+      g.elig_T1 = dd->Tr - 1;
+      g.top = dd->top16 + (size_t)dd->N * k;
+    }
+    if ((e = scb::tree_max_batch(tb, dd->Tr, dd->num_sms, stream, elem16)) != cudaSuccess)
+      return cuda_fail(e, "16-bit tree kernel");
+    if ((e = scb::flag_tiles_batch(pb, scb::tree_tile_width(), stream)) != cudaSuccess)
+      return cuda_fail(e, "flag kernel");
+    for (int k = 0; k < n; ++k) {
+      scb::TreeGroup& g = tb.g[k];
+      g.rows = inputs[k];
+      g.row_stride = strides[k];
+      g.top = b.s[k].top;
+      g.tile_list = pb.s[k].tile_list;
+      g.tile_count = pb.s[k].tile_count;
+    }
+    e = scb::tree_max_batch(tb, dd->Tr, dd->num_sms, stream, scb::kElemF32);
+  } else if (dd->Tr <= 16) {
     scb::TreeBatch tb;
     tb.count = n;
     tb.n_items = 0;
@@ -283,6 +396,11 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
   const long long nwin = ((long long)N + p.window_size - 1) / p.window_size;
   int rc = ensure_slots(dd, std::min(count, scb::kMaxBatch), (int)std::min<long long>(nwin + 1, N / 2 + 2));
   if (rc != SC_DD_OK) return rc;
+  const bool prec = dd->precision != SC_DD_PRECISION_FP32;
+  if (prec) {
+    if (Tr > 16) return fail(SC_DD_EINVAL, "the 16-bit forms support up to 16 rounded timesteps");
+    if ((rc = ensure_prec(dd, std::min(count, scb::kMaxBatch))) != SC_DD_OK) return rc;
+  }
   cudaError_t e;
   if ((e = cudaEventRecord(dd->ev[0], stream)) != cudaSuccess) return cuda_fail(e, "event");
   int total = 0;
@@ -298,6 +416,11 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
         (e = cudaMemcpy2DAsync(dd->host_cands(), sizeof(scb::Candidate) * kHostCands, dd->cands,
                                sizeof(scb::Candidate) * dd->cand_cap, sizeof(scb::Candidate) * head, n,
                                cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (prec && (e = cudaMemcpyAsync(dd->host_tile_counts, dd->tile_counts, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                                      stream)) != cudaSuccess) ||
+        (prec && k0 == 0 &&
+         (e = cudaMemcpyAsync(dd->host_norm, dd->norm_moments + 2 * scb::kVarChunks, sizeof(double) * 2,
+                              cudaMemcpyDeviceToHost, stream)) != cudaSuccess) ||
         (e = cudaStreamSynchronize(stream)) != cudaSuccess)
       return cuda_fail(e, "result copy");
     for (int k = 0; k < n; ++k) {
@@ -324,6 +447,11 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
         dd->last.min_drift_block = p.dmin;
         dd->last.max_drift_block = p.dmax;
         dd->last.num_candidates = ncand;
+        dd->last.precision = dd->precision;
+        dd->last.total_tiles = (N + scb::tree_tile_width() - 1) / scb::tree_tile_width();
+        dd->last.recomputed_tiles = prec ? dd->host_tile_counts[0] : dd->last.total_tiles;
+        dd->last.norm_mean = prec ? dd->host_norm[0] : 0.0;
+        dd->last.norm_std = prec ? dd->host_norm[1] : 0.0;
       }
       int nk = 0;
       for (const scb::Candidate& c : cands) {
@@ -479,6 +607,17 @@ int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_
   return SC_DD_OK;
 }
 
+int sc_dd_set_precision(sc_dd* dd, int precision) {
+  g_last_error.clear();
+  if (!dd) return fail(SC_DD_EINVAL, "sc_dd_set_precision: null engine");
+  if (precision != SC_DD_PRECISION_FP32 && precision != SC_DD_PRECISION_BF16 && precision != SC_DD_PRECISION_FP16)
+    return fail(SC_DD_EINVAL, "sc_dd_set_precision: unknown precision");
+  if (precision != SC_DD_PRECISION_FP32 && dd->Tr > 16)
+    return fail(SC_DD_EINVAL, "sc_dd_set_precision: the 16-bit forms support up to 16 rounded timesteps");
+  dd->precision = precision;
+  return SC_DD_OK;
+}
+
 int sc_dd_last_stats(const sc_dd* dd, sc_dd_stats* out) {
   if (!dd || !out) return fail(SC_DD_EINVAL, "sc_dd_last_stats: null argument");
   if (!dd->have_last) return fail(SC_DD_EINVAL, "sc_dd_last_stats: no search has completed");
@@ -487,11 +626,12 @@ int sc_dd_last_stats(const sc_dd* dd, sc_dd_stats* out) {
 }
 
 int sc_dd_copy_channel_array(sc_dd* dd, int which, float* dst, void* stream_ptr) {
-  if (!dd || !dst || (which != 0 && which != 1)) return fail(SC_DD_EINVAL, "sc_dd_copy_channel_array: bad argument");
+  if (!dd || !dst || which < 0 || which > 2) return fail(SC_DD_EINVAL, "sc_dd_copy_channel_array: bad argument");
   if (dd->slots < 1) return fail(SC_DD_EINVAL, "sc_dd_copy_channel_array: no scratch");
+  if (which == 2 && dd->prec_slots < 1) return fail(SC_DD_EINVAL, "sc_dd_copy_channel_array: no 16-bit search yet");
   DeviceGuard guard(dd->device);
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  const float* src = which == 0 ? dd->top : dd->colsum;
+  const float* src = which == 0 ? dd->top : (which == 1 ? dd->colsum : dd->top16);
   cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(float) * dd->N, cudaMemcpyDefault, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(e, "sc_dd_copy_channel_array");

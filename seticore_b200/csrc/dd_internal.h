@@ -10,6 +10,11 @@ constexpr int kMaxSeg = 4;       // staged windows per tree work item when jobs 
 constexpr int kMaxBatch = 64;    // searches per batched launch (descriptors travel as kernel parameters)
 constexpr int kVarChunks = 1024; // variance-emulation chunks per search, at most
 
+// Element types of a tree launch's input.
+constexpr int kElemF32 = 0;
+constexpr int kElemBF16 = 1;
+constexpr int kElemF16 = 2;
+
 // Radix-select state for the three column-sum order statistics (first, mid, last).
 struct SelectState {
   uint32_t prefix[3];
@@ -78,7 +83,7 @@ struct SearchBatch {
 // search and its in-block offset r is path offset off_base + k*off_step + r; eligibility
 // uses elig_T1 = rounded timesteps - 1.  The launcher fills the scheduling fields.
 struct TreeGroup {
-  const float* rows;
+  const void* rows;          // elements of the launch's element type
   long long row_stride;
   long long job_row_stride;  // 0: all jobs read the same rows (one shared trapezoid)
   int N;
@@ -91,6 +96,9 @@ struct TreeGroup {
   int off_step;
   int elig_T1;
   float* top;
+  // Optional: only the tiles listed in tile_list[0 .. *tile_count) (device memory).
+  const int* tile_list;
+  const int* tile_count;
   int jobs_per_chunk;
   int n_chunks;
   int n_tiles;
@@ -103,9 +111,37 @@ struct TreeBatch {
   TreeGroup g[kMaxBatch];
 };
 
-// Fused tree + per-channel top for the groups (all of R rows).  The launcher fills the
-// scheduling fields of `b` in place.
-cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream);
+// Fused tree + per-channel top for the groups (all of R rows, elements of type `elem`).
+// The launcher fills the scheduling fields of `b` in place.
+cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream, int elem = kElemF32);
+
+// Channels per tree work item (the tile a flag refers to).
+int tree_tile_width();
+
+// Precision form (dd_precision.cu), per search of a batch:
+struct PrecisionDesc {
+  const float* input;   // original float32 power [Tr][N], row stride row_stride
+  long long row_stride;
+  int T, Tr, N;         // unrounded and rounded timesteps, channels
+  void* norm;           // normalised 16-bit copy [Tr][N] (dense)
+  double* moments;      // 2 * kVarChunks partial sums + [mean, std] at 2 * kVarChunks
+  unsigned* ticket;
+  const float* top16;   // tops of the 16-bit tree (normalised units)
+  const SearchHeader* hdr;
+  double snr_threshold;
+  int* tile_list;       // flagged tiles
+  int* tile_count;
+};
+struct PrecisionBatch {
+  int count;
+  int maxN;
+  int elem;             // kElemBF16 or kElemF16
+  PrecisionDesc s[kMaxBatch];
+};
+// FP64 mean and standard deviation of the unrounded rows, then the normalised copy.
+cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
+// Flags every tile holding a channel whose 16-bit top reaches 0.9 x the threshold.
+cudaError_t flag_tiles_batch(const PrecisionBatch& b, int tile_width, cudaStream_t stream);
 
 // Column sums, order statistics, mean, standard deviation and threshold of each search.
 cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);

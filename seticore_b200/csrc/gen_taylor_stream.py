@@ -140,8 +140,8 @@ def gen_strip_loop(R, lo, hi, U, ITERS):
     lines += carry
     lines.append("  }")
     body_text = "\n".join(lines)
-    return (f"template <>\n__device__ __forceinline__ void taylor_strip_loop<{R}, {lo}, {hi}, {U}, {ITERS}>(\n"
-            f"    const float* const (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
+    return (f"template <typename Row>\n__device__ __forceinline__ void taylor_strip_loop_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
+            f"    const Row (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
 
 
 # (R, offset parts, U steps per iteration, iterations) compiled into the library; a strip is
@@ -150,15 +150,21 @@ LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3)]
 
 
 def main(out_path):
-    parts = [
-        "// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n",
-        "template <int R, int LO, int HI, int U, int ITERS>\n"
-        "__device__ __forceinline__ void taylor_strip_loop(const float* const (&row)[R], float* __restrict__ mrow);\n",
-    ]
+    parts = ["// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n"]
     for R, nparts, U, IT in LOOP_CONFIGS:
         step = R // nparts
         for k in range(nparts):
             parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT))
+    # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS>(row, mrow) for any element accessor.
+    parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row>\n"
+                 "__device__ __forceinline__ void taylor_strip_loop(const Row (&row)[R], float* __restrict__ mrow) {")
+    for R, nparts, U, IT in LOOP_CONFIGS:
+        step = R // nparts
+        for k in range(nparts):
+            lo, hi = k * step, (k + 1) * step
+            parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT}) "
+                         f"taylor_strip_loop_{R}_{lo}_{hi}_{U}_{IT}(row, mrow);")
+    parts.append("}")
     text = "\n".join(parts)
     if os.path.exists(out_path) and open(out_path).read() == text:
         return

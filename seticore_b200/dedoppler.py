@@ -197,6 +197,14 @@ class Dedopplerer:
         except Exception:
             pass
 
+    def set_precision(self, precision: str) -> None:
+        """'fp32' (the reference's form), 'bf16' or 'fp16' (normalised 16-bit storage with
+        exact FP32 recomputation near the threshold; identical hit lists)."""
+        code = {"fp32": _capi.SC_DD_PRECISION_FP32, "bf16": _capi.SC_DD_PRECISION_BF16,
+                "fp16": _capi.SC_DD_PRECISION_FP16}[precision]
+        check(lib().sc_dd_set_precision(self._h, code))
+        self.precision = precision
+
     def memoryUsage(self) -> int:
         return int(lib().sc_dd_memory_usage(self._h))
 
@@ -298,6 +306,6 @@ class Dedopplerer:
         """Copy of the last search's per-channel 'top' path sums or 'colsum' column sums."""
         import torch
         out = torch.empty(self.num_channels, dtype=torch.float32, device="cuda")
-        check(lib().sc_dd_copy_channel_array(self._h, 0 if which == "top" else 1,
+        check(lib().sc_dd_copy_channel_array(self._h, {"top": 0, "colsum": 1, "top16": 2}[which],
                                              ctypes.c_void_p(out.data_ptr()), _stream_handle(None)))
         return out

@@ -1,0 +1,93 @@
+"""The precision form: 16-bit normalised storage with exact FP32 recomputation.
+
+Bar: the BF16 and FP16 forms return exactly the FP32 form's hit list (index, drift,
+power bit-for-bit, SNR); the approximate path sums they compute are compared with the
+FP64 oracle (tree in double precision, same geometry) and the error is stated.
+"""
+import numpy as np
+import pytest
+
+from tests.conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    import torch
+    return torch
+
+
+def _hits(dd, xt, spec):
+    return [(h.index, h.drift_steps, np.float32(h.power), np.float32(h.snr))
+            for h in dd.search_raw(xt, -1, 0, spec.max_drift, spec.min_drift, spec.snr_threshold)]
+
+
+CASES = [(16, 65536, 4.0, 1, 1), (16, 40000, 4.0, 2, 0), (8, 30000, 2.0, 3, 2), (13, 20000, 3.0, 4, 1),
+         (4, 50000, 1.0, 5, 1), (2, 20000, 1.0, 6, 0), (16, 1 << 20, 4.0, 7, 2)]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"T{c[0]}_N{c[1]}_s{c[3]}")
+@pytest.mark.parametrize("precision", ["bf16", "fp16"])
+def test_16bit_forms_return_the_fp32_hit_list(torch_cuda, case, precision):
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    T, N, md, seed, spikes = case
+    spec = SearchSpec(T, N, max_drift=md, seed=900 + seed, n_tones=8, n_spikes=spikes, tone_drift=min(md, 4.0),
+                      tsamp=18.253611 * 16 / max(T, 16), snr_threshold=8.0)
+    xt = torch_cuda.from_numpy(make_filterbank_numpy(spec)).cuda()
+    dd = Dedopplerer(T, N, spec.foff_mhz, spec.tsamp)
+    want = _hits(dd, xt, spec)
+    dd.set_precision(precision)
+    got = _hits(dd, xt, spec)
+    st = dd.last_stats()
+    assert got == want
+    assert len(want) >= 1
+    assert 0 < st.recomputed_tiles <= st.total_tiles
+    # a second call on the same engine (scratch reuse) gives the same answer
+    assert _hits(dd, xt, spec) == want
+    dd.close()
+
+
+def _fp64_top(oracle, x, spec):
+    """Per-channel maximum over eligible paths (the reference's rule), FP64 tree."""
+    Tr, N = x.shape
+    res = 1e6 * spec.foff_mhz / ((Tr - 1) * spec.tsamp)
+    nmax = spec.max_drift / abs(res * (Tr - 1))
+    top = np.zeros(N)
+    c = np.arange(N)
+    for db in range(int(np.floor(-nmax)), int(np.floor(nmax)) + 1):
+        out = oracle.taylor_f64(x, db)
+        e = (Tr - 1) * db
+        for off in range(Tr):
+            ok = (c + e >= 0) & (c + e + off < N)
+            v = np.where(ok, out[off], -np.inf)
+            top = np.maximum(top, np.nan_to_num(v, nan=-np.inf))
+    return top
+
+
+def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle):
+    """States the top-path-sum error of each form against the FP64 tree (printed), and
+    bounds it: FP32 1e-6, FP16 1e-3, BF16 1e-2 relative (to the top sum)."""
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    spec = SearchSpec(16, 32768, seed=77, n_tones=8, snr_threshold=8.0)
+    x = make_filterbank_numpy(spec)
+    ref = _fp64_top(port_oracle, x, spec)
+    xt = torch_cuda.from_numpy(x).cuda()
+    dd = Dedopplerer(16, spec.num_channels, spec.foff_mhz, spec.tsamp)
+    dd.search_raw(xt, -1, 0, spec.max_drift, 0.0, spec.snr_threshold)
+    top32 = dd.channel_array("top").cpu().numpy().astype(np.float64)
+    err = {"fp32": np.max(np.abs(top32 - ref) / ref)}
+    for prec, bound in (("fp16", 1e-3), ("bf16", 1e-2)):
+        dd.set_precision(prec)
+        dd.search_raw(xt, -1, 0, spec.max_drift, 0.0, spec.snr_threshold)
+        st = dd.last_stats()
+        approx = dd.channel_array("top16").cpu().numpy().astype(np.float64) * st.norm_std + 16 * st.norm_mean
+        sel = ref > np.percentile(ref, 50)  # the approximate tops are floored at 0 in normalised units
+        err[prec] = np.max(np.abs(approx[sel] - ref[sel]) / ref[sel])
+        assert err[prec] < bound, (prec, err[prec])
+    print("max relative top-path-sum error vs FP64:", err)
+    assert err["fp32"] < 1e-6
