@@ -175,6 +175,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--fp32-only", action="store_true", help="skip the BF16/FP16 precision-form lines")
     ap.add_argument("--coarse", type=int, default=N_COARSE,
                     help="coarse channels per node (64; fewer only for small profiling captures)")
     args = ap.parse_args()
@@ -229,6 +230,34 @@ def main():
     ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
     samples_per_step = n_coarse * T * N
     value = world * samples_per_step / (ms / 1e3) / 1e9
+
+    # The precision forms on the same node: identical hit lists required.
+    ref_hits = dd.search_batch_raw(inputs, beams, coarse, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+    ref_key = [[(h.index, h.drift_steps, h.power) for h in hs] for hs in ref_hits]
+    precision = {}
+    for prec in ([] if args.fp32_only else ["bf16", "fp16"]):
+        dd.set_precision(prec)
+        for _ in range(max(3, args.warmup)):
+            got = dd.search_batch_raw(inputs, beams, coarse, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+        identical = [[(h.index, h.drift_steps, h.power) for h in hs] for hs in got] == ref_key
+        barrier(world)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        ptree = []
+        for _ in range(args.steps):
+            dd.search_batch_raw(inputs, beams, coarse, MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+            ptree.append(dd.last_stats().tree_ms)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        st = dd.last_stats()
+        p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
+        precision[prec] = {"value": world * samples_per_step / (p_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": p_ms,
+                           "hits_identical_to_fp32": identical,
+                           "recomputed_tiles_first_search": f"{st.recomputed_tiles}/{st.total_tiles}",
+                           "speedup_vs_fp32": ms / p_ms}
+    dd.set_precision("fp32")
 
     # End to end through the public API: host (pinned) -> device copies inside the timing,
     # in chunks of E2E_CHUNK coarse channels; the copy of chunk j+1 overlaps the search of j.
@@ -307,6 +336,7 @@ def main():
                                    "channel, max_drift 4 Hz/s, snr 10", "drift_blocks": ndb,
                        "l2": "inputs (4.3 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
             "clocks": clk, "roofline": roofline, "e2e": e2e,
+            "precision_forms": precision,
             "gpu_launches": len(tree_ms) * 12 * ((n_coarse + 63) // 64),
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
