@@ -142,6 +142,59 @@ const char* sc_dd_last_error(void);
 /* Library version string. */
 const char* sc_dd_version(void);
 
+/* ---- Heterogeneous batches: many searches of different shapes at once ---- */
+
+/* One search request: its input, the shape sc_dd_create would take, and the arguments
+ * of Dedopplerer::search (dedoppler.h:42-45), plus its storage precision. */
+typedef struct sc_dd_request {
+  const float* dev_input; /* [rounded T][N] float32, row_stride elements between rows */
+  long long row_stride;
+  int num_timesteps;      /* unrounded */
+  int num_channels;
+  double foff_mhz;
+  double tsamp_s;
+  double max_drift;
+  double min_drift;
+  double snr_threshold;
+  int beam;
+  int coarse_channel;
+  int precision;          /* SC_DD_PRECISION_* */
+  int pad;
+} sc_dd_request;
+
+typedef struct sc_dd_pool_stats {
+  long long calls;
+  long long sub_batches;     /* admitted groups of requests that fit the scratch budget */
+  long long graph_replays;   /* sub-batches replayed from a captured CUDA graph */
+  long long graph_captures;
+  long long tuned_launches;  /* autotuning decisions taken (tree launches, level splits) */
+  float last_call_ms;        /* device time of the last call, CUDA events */
+  int pad;
+} sc_dd_pool_stats;
+
+typedef struct sc_dd_pool sc_dd_pool;
+
+/* A pool runs lists of requests of any mix of shapes: requests are admitted in order
+ * into sub-batches whose scratch fits scratch_budget_bytes (one request always fits:
+ * the pool grows its arena for a larger one), every kernel runs once per sub-batch of up
+ * to 64 searches, tree launches and level splits are autotuned on first sight, and a
+ * sub-batch seen again is replayed from a captured CUDA graph.  No counterpart in the
+ * reference (which runs one search at a time). */
+int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out);
+int sc_dd_pool_destroy(sc_dd_pool* pool);
+/* autotune / cuda_graphs: 1 (default) or 0. */
+int sc_dd_pool_configure(sc_dd_pool* pool, int autotune, int cuda_graphs);
+/* Runs the requests; hits are written request after request (each in increasing index
+ * order) and num_hits[i] receives request i's count.  Returns after the hits are on the
+ * host; work is ordered on `stream`. */
+int sc_dd_pool_search(sc_dd_pool* pool, const sc_dd_request* requests, int count,
+                      sc_dd_hit* out, int capacity, int* num_hits, void* stream);
+int sc_dd_pool_stats_get(const sc_dd_pool* pool, sc_dd_pool_stats* out);
+/* Device scratch bytes one request needs in a pool (0 for an invalid request). */
+size_t sc_dd_request_scratch_bytes(const sc_dd_request* request);
+/* Message of the calling thread's last failed pool call. */
+const char* sc_dd_pool_last_error(void);
+
 /* Largest channel count sc_dd_search_static accepts. */
 #define SC_DD_STATIC_MAX_CHANNELS 1048576
 

@@ -28,7 +28,39 @@ EXPORTED = [
     "sc_dd_search", "sc_dd_search_batch", "sc_dd_add_incoherent_power", "sc_dd_set_precision",
     "sc_dd_last_stats",
     "sc_dd_copy_channel_array", "sc_dd_last_error", "sc_dd_version", "sc_dd_search_static",
+    "sc_dd_pool_create", "sc_dd_pool_destroy", "sc_dd_pool_configure", "sc_dd_pool_search",
+    "sc_dd_pool_stats_get", "sc_dd_request_scratch_bytes", "sc_dd_pool_last_error",
 ]
+
+
+class ScDdRequest(ctypes.Structure):
+    _fields_ = [
+        ("dev_input", ctypes.c_void_p),
+        ("row_stride", ctypes.c_longlong),
+        ("num_timesteps", ctypes.c_int),
+        ("num_channels", ctypes.c_int),
+        ("foff_mhz", ctypes.c_double),
+        ("tsamp_s", ctypes.c_double),
+        ("max_drift", ctypes.c_double),
+        ("min_drift", ctypes.c_double),
+        ("snr_threshold", ctypes.c_double),
+        ("beam", ctypes.c_int),
+        ("coarse_channel", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("pad", ctypes.c_int),
+    ]
+
+
+class ScDdPoolStats(ctypes.Structure):
+    _fields_ = [
+        ("calls", ctypes.c_longlong),
+        ("sub_batches", ctypes.c_longlong),
+        ("graph_replays", ctypes.c_longlong),
+        ("graph_captures", ctypes.c_longlong),
+        ("tuned_launches", ctypes.c_longlong),
+        ("last_call_ms", ctypes.c_float),
+        ("pad", ctypes.c_int),
+    ]
 
 
 class ScDdHit(ctypes.Structure):
@@ -96,6 +128,15 @@ def lib():
         L.sc_dd_add_incoherent_power.argtypes = [vp, vp, ll, ctypes.POINTER(ScDdHit), i, vp]
         L.sc_dd_last_stats.argtypes = [vp, ctypes.POINTER(ScDdStats)]
         L.sc_dd_set_precision.argtypes = [vp, i]
+        L.sc_dd_pool_create.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.sc_dd_pool_destroy.argtypes = [vp]
+        L.sc_dd_pool_configure.argtypes = [vp, i, i]
+        L.sc_dd_pool_search.argtypes = [vp, ctypes.POINTER(ScDdRequest), i, ctypes.POINTER(ScDdHit), i,
+                                        ctypes.POINTER(i), vp]
+        L.sc_dd_pool_stats_get.argtypes = [vp, ctypes.POINTER(ScDdPoolStats)]
+        L.sc_dd_request_scratch_bytes.argtypes = [ctypes.POINTER(ScDdRequest)]
+        L.sc_dd_request_scratch_bytes.restype = ctypes.c_size_t
+        L.sc_dd_pool_last_error.restype = ctypes.c_char_p
         L.sc_dd_search_static.argtypes = [vp, ll, i, i, d, d, i, i, d, d, d, ctypes.POINTER(ScDdHit), i,
                                           ctypes.POINTER(i), vp]
         L.sc_dd_copy_channel_array.argtypes = [vp, i, vp, vp]
@@ -110,7 +151,8 @@ def lib():
     return _lib
 
 
-def check(rc):
+def check(rc, pool=False):
     if rc != SC_DD_OK:
-        raise DedopplerError(rc, lib().sc_dd_last_error().decode())
+        msg = (lib().sc_dd_pool_last_error() if pool else lib().sc_dd_last_error()).decode()
+        raise DedopplerError(rc, msg)
     return rc

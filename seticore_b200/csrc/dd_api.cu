@@ -278,109 +278,61 @@ scb::SearchDesc make_desc(sc_dd* d, int slot, const float* input, long long row_
 }
 
 // Queues n <= kMaxBatch searches into slots 0..n-1.
+struct EventHooks {
+  sc_dd* dd;
+  bool record;
+};
+
 int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* strides, const DriftPlan& p,
                 double snr_threshold, cudaStream_t stream, bool first_batch) {
-  scb::SearchBatch b;
-  b.count = n;
-  b.maxN = dd->N;
-  for (int k = 0; k < n; ++k) b.s[k] = make_desc(dd, k, inputs[k], strides[k], p, snr_threshold);
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(dd->top, 0, sizeof(float) * dd->N * (size_t)n, stream)) != cudaSuccess ||
-      (e = cudaMemsetAsync(dd->hdrs, 0, sizeof(scb::SearchHeader) * n, stream)) != cudaSuccess)
-    return cuda_fail(e, "memset");
+  scb::ExecSearch es[scb::kMaxBatch];
   const bool prec = dd->precision != SC_DD_PRECISION_FP32;
-  const int elem16 = dd->precision == SC_DD_PRECISION_BF16 ? scb::kElemBF16 : scb::kElemF16;
-  scb::PrecisionBatch pb;
-  if (prec) {
-    pb.count = n;
-    pb.maxN = dd->N;
-    pb.elem = elem16;
-    for (int k = 0; k < n; ++k) {
-      scb::PrecisionDesc& q = pb.s[k];
-      q.input = inputs[k];
-      q.row_stride = strides[k];
-      q.T = dd->T;
-      q.Tr = dd->Tr;
-      q.N = dd->N;
-      q.norm = static_cast<char*>(dd->norm16) + (size_t)2 * dd->N * dd->Tr * k;
-      q.moments = dd->norm_moments + (size_t)(2 * scb::kVarChunks + 2) * k;
-      q.ticket = dd->norm_tickets + k;
-      q.top16 = dd->top16 + (size_t)dd->N * k;
-      q.hdr = b.s[k].hdr;
-      q.snr_threshold = snr_threshold;
-      q.tile_list = dd->tiles + (size_t)dd->max_tiles * k;
+  const int elem = !prec ? scb::kElemF32
+                         : (dd->precision == SC_DD_PRECISION_BF16 ? scb::kElemBF16 : scb::kElemF16);
+  for (int k = 0; k < n; ++k) {
+    scb::ExecSearch& q = es[k];
+    q = scb::ExecSearch{};
+    q.input = inputs[k];
+    q.row_stride = strides[k];
+    q.T = dd->T;
+    q.Tr = dd->Tr;
+    q.N = dd->N;
+    q.dmin = p.dmin;
+    q.dmax = p.dmax;
+    q.window_size = p.window_size;
+    q.snr_threshold = snr_threshold;
+    q.elem = elem;
+    q.cand_cap = dd->cand_cap;
+    const size_t N = dd->N;
+    q.top = dd->top + N * k;
+    q.colsum = dd->colsum + N * k;
+    q.sel = dd->sel + k;
+    q.partials = dd->partials + (size_t)dd->n_partials * k;
+    q.var = dd->var + (size_t)2 * scb::kVarChunks * k;
+    q.hdr = dd->hdrs + k;
+    q.cands = dd->cands + (size_t)dd->cand_cap * k;
+    if (prec) {
+      q.norm16 = static_cast<char*>(dd->norm16) + (size_t)2 * dd->N * dd->Tr * k;
+      q.top16 = dd->top16 + N * k;
+      q.tiles = dd->tiles + (size_t)dd->max_tiles * k;
       q.tile_count = dd->tile_counts + k;
+      q.norm_moments = dd->norm_moments + (size_t)(2 * scb::kVarChunks + 2) * k;
+      q.norm_ticket = dd->norm_tickets + k;
     }
-    if ((e = cudaMemsetAsync(dd->top16, 0, sizeof(float) * dd->N * (size_t)n, stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(dd->tile_counts, 0, sizeof(int) * n, stream)) != cudaSuccess)
-      return cuda_fail(e, "memset");
-    if ((e = scb::normalize_batch(pb, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "normalisation kernels");
   }
-  if ((e = scb::search_stats_batch(b, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "statistics kernels");
-  if (first_batch) cudaEventRecord(dd->ev[1], stream);
-  if (prec) {
-    // Approximate tops over the 16-bit copy, flags, then exact FP32 tops of flagged tiles.
-    scb::TreeBatch tb;
-    tb.count = n;
-    tb.n_items = 0;
-    for (int k = 0; k < n; ++k) {
-      scb::TreeGroup& g = tb.g[k];
-      g = scb::TreeGroup{};
-      g.rows = pb.s[k].norm;
-      g.row_stride = dd->N;
-      g.N = dd->N;
-      g.d_first = p.dmin;
-      g.d_step = 1;
-      g.n_jobs = p.dmax - p.dmin + 1;
-      g.db_first = p.dmin;
-      g.db_step = 1;
-      g.elig_T1 = dd->Tr - 1;
-      g.top = dd->top16 + (size_t)dd->N * k;
-    }
-    if ((e = scb::tree_max_batch(tb, dd->Tr, dd->num_sms, stream, elem16)) != cudaSuccess)
-      return cuda_fail(e, "16-bit tree kernel");
-    if ((e = scb::flag_tiles_batch(pb, scb::tree_tile_width(), stream)) != cudaSuccess)
-      return cuda_fail(e, "flag kernel");
-    for (int k = 0; k < n; ++k) {
-      scb::TreeGroup& g = tb.g[k];
-      g.rows = inputs[k];
-      g.row_stride = strides[k];
-      g.top = b.s[k].top;
-      g.tile_list = pb.s[k].tile_list;
-      g.tile_count = pb.s[k].tile_count;
-    }
-    e = scb::tree_max_batch(tb, dd->Tr, dd->num_sms, stream, scb::kElemF32);
-  } else if (dd->Tr <= 16) {
-    scb::TreeBatch tb;
-    tb.count = n;
-    tb.n_items = 0;
-    for (int k = 0; k < n; ++k) {
-      scb::TreeGroup& g = tb.g[k];
-      g = scb::TreeGroup{};
-      g.rows = inputs[k];
-      g.row_stride = strides[k];
-      g.job_row_stride = 0;
-      g.N = dd->N;
-      g.d_first = p.dmin;
-      g.d_step = 1;
-      g.n_jobs = p.dmax - p.dmin + 1;
-      g.db_first = p.dmin;
-      g.db_step = 1;
-      g.off_base = 0;
-      g.off_step = 0;
-      g.elig_T1 = dd->Tr - 1;
-      g.top = b.s[k].top;
-    }
-    e = scb::tree_max_batch(tb, dd->Tr, dd->num_sms, stream);
-  } else {
-    e = cudaSuccess;
-    for (int k = 0; k < n && e == cudaSuccess; ++k)
-      e = scb::levels_search(inputs[k], strides[k], dd->Tr, dd->N, p.dmin, p.dmax, dd->scratch_a, dd->scratch_b,
-                             b.s[k].top, dd->num_sms, stream);
-  }
-  if (e != cudaSuccess) return cuda_fail(e, "tree kernels");
-  if (first_batch) cudaEventRecord(dd->ev[2], stream);
-  if ((e = scb::search_hits_batch(b, dd->num_sms, stream)) != cudaSuccess) return cuda_fail(e, "hit kernels");
+  EventHooks eh{dd, first_batch};
+  scb::ExecHooks hooks;
+  hooks.ctx = &eh;
+  hooks.after_stats = [](void* c, cudaStream_t st) {
+    EventHooks* h = static_cast<EventHooks*>(c);
+    if (h->record) cudaEventRecord(h->dd->ev[1], st);
+  };
+  hooks.after_tree = [](void* c, cudaStream_t st) {
+    EventHooks* h = static_cast<EventHooks*>(c);
+    if (h->record) cudaEventRecord(h->dd->ev[2], st);
+  };
+  cudaError_t e = scb::exec_queue(es, n, dd->scratch_a, dd->scratch_b, dd->num_sms, stream, hooks);
+  if (e != cudaSuccess) return cuda_fail(e, "search kernels");
   return SC_DD_OK;
 }
 

@@ -1,0 +1,245 @@
+// Queues the kernels of a list of searches of any shapes, drift ranges and precisions.
+//
+// Used by the engine (dd_api.cu, one shape) and by the pool (dd_pool.cu, mixed shapes).
+// The searches travel in batches of up to kMaxBatch as kernel parameters, so a call is a
+// fixed sequence of launches (capturable in a CUDA graph) whatever the mix:
+//   clear -> [normalise] -> statistics -> tree launches grouped by (rows, element type)
+//   (levels for more than 16 rows, one search at a time) -> [flag + FP32 recompute] -> hits
+#include <algorithm>
+
+#include "dd_common.cuh"
+#include "dd_internal.h"
+
+namespace scb {
+
+namespace {
+
+// Zeroes, per search of the batch: top (and the 16-bit tops), the result header and the
+// flagged-tile count.
+__global__ void clear_kernel(const __grid_constant__ SearchBatch b, const __grid_constant__ PrecisionBatch pb) {
+  const SearchDesc& d = b.s[blockIdx.y];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) d.top[c] = 0.0f;
+  if (blockIdx.x == 0 && threadIdx.x < (int)(sizeof(SearchHeader) / 4))
+    reinterpret_cast<int*>(d.hdr)[threadIdx.x] = 0;
+  if (pb.count > 0 && blockIdx.y < (unsigned)pb.count && pb.s[blockIdx.y].tile_count) {
+    const PrecisionDesc& q = pb.s[blockIdx.y];
+    float* t16 = const_cast<float*>(q.top16);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < q.N; c += gridDim.x * blockDim.x) t16[c] = 0.0f;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      *q.tile_count = 0;
+      *q.ticket = 0;
+    }
+  }
+}
+
+SearchDesc to_desc(const ExecSearch& e) {
+  SearchDesc s{};
+  s.input = e.input;
+  s.row_stride = e.row_stride;
+  s.Tr = e.Tr;
+  s.N = e.N;
+  s.dmin = e.dmin;
+  s.dmax = e.dmax;
+  s.window_size = e.window_size;
+  s.first = (int)ceil(0.05 * e.N);  // dedoppler.cu:327
+  s.mid = e.N / 2;                   // dedoppler.cu:291
+  s.last = (int)floor(0.95 * e.N);  // dedoppler.cu:328
+  s.snr_threshold = e.snr_threshold;
+  s.top = e.top;
+  s.colsum = e.colsum;
+  s.sel = e.sel;
+  s.partials = e.partials;
+  s.var = e.var;
+  s.hdr = e.hdr;
+  s.cands = e.cands;
+  s.cand_cap = e.cand_cap;
+  return s;
+}
+
+PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
+  PrecisionDesc q{};
+  q.input = e.input;
+  q.row_stride = e.row_stride;
+  q.T = e.T;
+  q.Tr = e.Tr;
+  q.N = e.N;
+  q.norm = e.norm16;
+  q.moments = e.norm_moments;
+  q.ticket = e.norm_ticket;
+  q.top16 = e.top16;
+  q.hdr = hdr;
+  q.snr_threshold = e.snr_threshold;
+  q.tile_list = e.tiles;
+  q.tile_count = e.tile_count;
+  return q;
+}
+
+TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride, float* top) {
+  TreeGroup g{};
+  g.rows = rows;
+  g.row_stride = row_stride;
+  g.job_row_stride = 0;
+  g.N = e.N;
+  g.d_first = e.dmin;
+  g.d_step = 1;
+  g.n_jobs = e.dmax - e.dmin + 1;
+  g.db_first = e.dmin;
+  g.db_step = 1;
+  g.off_base = 0;
+  g.off_step = 0;
+  g.elig_T1 = e.Tr - 1;
+  g.top = top;
+  return g;
+}
+
+}  // namespace
+
+cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
+                       const ExecHooks& hooks) {
+  cudaError_t e = cudaSuccess;
+  for (int k0 = 0; k0 < n && e == cudaSuccess; k0 += kMaxBatch) {
+    const int m = std::min(kMaxBatch, n - k0);
+    const ExecSearch* ss = s + k0;
+    SearchBatch b;
+    b.count = m;
+    b.maxN = 0;
+    for (int k = 0; k < m; ++k) {
+      b.s[k] = to_desc(ss[k]);
+      b.maxN = std::max(b.maxN, ss[k].N);
+    }
+    // Clear (one launch).
+    PrecisionBatch clear_pb;
+    clear_pb.count = m;
+    clear_pb.maxN = b.maxN;
+    clear_pb.elem = kElemBF16;
+    for (int k = 0; k < m; ++k) {
+      clear_pb.s[k] = PrecisionDesc{};
+      if (ss[k].elem != kElemF32) clear_pb.s[k] = to_pdesc(ss[k], b.s[k].hdr);
+    }
+    {
+      int gx = (b.maxN + 1023) / 1024;
+      if (gx > 64) gx = 64;
+      clear_kernel<<<dim3(gx, m), 256, 0, stream>>>(b, clear_pb);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // Normalisation of the 16-bit searches (one launch per element type).
+    for (int elem : {kElemBF16, kElemF16}) {
+      PrecisionBatch q;
+      q.count = 0;
+      q.maxN = 0;
+      q.elem = elem;
+      for (int k = 0; k < m; ++k)
+        if (ss[k].elem == elem) {
+          q.s[q.count++] = to_pdesc(ss[k], b.s[k].hdr);
+          q.maxN = std::max(q.maxN, ss[k].N);
+        }
+      if (q.count && (e = normalize_batch(q, num_sms, stream)) != cudaSuccess) return e;
+    }
+    if ((e = search_stats_batch(b, num_sms, stream)) != cudaSuccess) return e;
+    if (hooks.after_stats) hooks.after_stats(hooks.ctx, stream);
+    // Trees over up to 16 rows: one launch per (rows, element type).
+    for (int R : {2, 4, 8, 16}) {
+      for (int elem : {kElemF32, kElemBF16, kElemF16}) {
+        TreeBatch tb;
+        tb.count = 0;
+        tb.n_items = 0;
+        for (int k = 0; k < m; ++k) {
+          if (ss[k].Tr != R || ss[k].elem != elem) continue;
+          if (elem == kElemF32) tb.g[tb.count++] = tree_group(ss[k], ss[k].input, ss[k].row_stride, ss[k].top);
+          else tb.g[tb.count++] = tree_group(ss[k], ss[k].norm16, ss[k].N, ss[k].top16);
+        }
+        if (tb.count && (e = tree_max_batch(tb, R, num_sms, stream, elem, hooks.budget_kb(hooks.ctx, tb, R, elem))) !=
+                            cudaSuccess)
+          return e;
+      }
+    }
+    // More than 16 rows: the level path, one search at a time (shared level buffers).
+    for (int k = 0; k < m; ++k) {
+      if (ss[k].Tr <= 16) continue;
+      const LevelPlan plan = hooks.level_plan ? hooks.level_plan(hooks.ctx, ss[k], lvl_a, lvl_b, stream) : ss[k].level_plan;
+      if ((e = levels_search(ss[k].input, ss[k].row_stride, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
+                             ss[k].top, num_sms, stream, plan)) != cudaSuccess)
+        return e;
+    }
+    // The 16-bit searches: flag tiles near the threshold, recompute them exactly in FP32.
+    {
+      PrecisionBatch q;
+      q.count = 0;
+      q.maxN = 0;
+      q.elem = kElemBF16;
+      for (int k = 0; k < m; ++k)
+        if (ss[k].elem != kElemF32) {
+          q.s[q.count++] = to_pdesc(ss[k], b.s[k].hdr);
+          q.maxN = std::max(q.maxN, ss[k].N);
+        }
+      if (q.count) {
+        if ((e = flag_tiles_batch(q, tree_tile_width(), stream)) != cudaSuccess) return e;
+        for (int R : {2, 4, 8, 16}) {
+          TreeBatch tb;
+          tb.count = 0;
+          tb.n_items = 0;
+          for (int k = 0; k < m; ++k) {
+            if (ss[k].Tr != R || ss[k].elem == kElemF32) continue;
+            TreeGroup g = tree_group(ss[k], ss[k].input, ss[k].row_stride, ss[k].top);
+            g.tile_list = ss[k].tiles;
+            g.tile_count = ss[k].tile_count;
+            tb.g[tb.count++] = g;
+          }
+          if (tb.count && (e = tree_max_batch(tb, R, num_sms, stream, kElemF32,
+                                              hooks.budget_kb(hooks.ctx, tb, R, kElemF32))) != cudaSuccess)
+            return e;
+        }
+      }
+    }
+    if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);
+    if ((e = search_hits_batch(b, num_sms, stream)) != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
+size_t ExecSearch::scratch_bytes(int Tr, int N, int cand_cap, int n_partials, int elem) {
+  auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
+  size_t b = a(sizeof(float) * N) * 2 + a(sizeof(SelectState)) + a(sizeof(MomentPartial) * n_partials) +
+             a(sizeof(double) * 2 * kVarChunks) + a(sizeof(SearchHeader)) + a(sizeof(Candidate) * cand_cap);
+  if (elem != kElemF32) {
+    const int tiles = (N + tree_tile_width() - 1) / tree_tile_width();
+    b += a((size_t)2 * Tr * N) + a(sizeof(float) * N) + a(sizeof(int) * tiles) + a(sizeof(int)) +
+         a(sizeof(double) * (2 * kVarChunks + 2)) + a(sizeof(unsigned));
+  }
+  return b;
+}
+
+void ExecSearch::carve(char* base, int n_partials) {
+  auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
+  char* p = base;
+  top = reinterpret_cast<float*>(p);
+  p += a(sizeof(float) * N);
+  colsum = reinterpret_cast<float*>(p);
+  p += a(sizeof(float) * N);
+  sel = reinterpret_cast<SelectState*>(p);
+  p += a(sizeof(SelectState));
+  partials = reinterpret_cast<MomentPartial*>(p);
+  p += a(sizeof(MomentPartial) * n_partials);
+  var = reinterpret_cast<double*>(p);
+  p += a(sizeof(double) * 2 * kVarChunks);
+  hdr = reinterpret_cast<SearchHeader*>(p);
+  p += a(sizeof(SearchHeader));
+  cands = reinterpret_cast<Candidate*>(p);
+  p += a(sizeof(Candidate) * cand_cap);
+  if (elem != kElemF32) {
+    const int tiles_n = (N + tree_tile_width() - 1) / tree_tile_width();
+    norm16 = p;
+    p += a((size_t)2 * Tr * N);
+    top16 = reinterpret_cast<float*>(p);
+    p += a(sizeof(float) * N);
+    tiles = reinterpret_cast<int*>(p);
+    p += a(sizeof(int) * tiles_n);
+    tile_count = reinterpret_cast<int*>(p);
+    p += a(sizeof(int));
+    norm_moments = reinterpret_cast<double*>(p);
+    p += a(sizeof(double) * (2 * kVarChunks + 2));
+    norm_ticket = reinterpret_cast<unsigned*>(p);
+  }
+}
+
+}  // namespace scb

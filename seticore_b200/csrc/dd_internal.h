@@ -112,8 +112,11 @@ struct TreeBatch {
 };
 
 // Fused tree + per-channel top for the groups (all of R rows, elements of type `elem`).
-// The launcher fills the scheduling fields of `b` in place.
-cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream, int elem = kElemF32);
+// The launcher fills the scheduling fields of `b` in place.  smem_budget_kb bounds the
+// shared memory of a CTA (0: the default), which sets how many drift blocks share a staged
+// trapezoid and how many CTAs fit an SM.
+cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream, int elem = kElemF32,
+                           int smem_budget_kb = 0);
 
 // Channels per tree work item (the tile a flag refers to).
 int tree_tile_width();
@@ -153,11 +156,65 @@ cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t st
 cudaError_t path_values(const float* input, long long row_stride, int Tr, int N, const int* index,
                         const int* drift_steps, float* out, int n, cudaStream_t stream);
 
+// How a tree of more than 16 rows is split: emit levels of m[0..n) rows (2 or 4 each),
+// then a fused max level of final_rows (2, 4, 8 or 16) rows.  n == 0: the default split.
+struct LevelPlan {
+  int n;
+  int m[12];
+  int final_rows;
+};
+
 // Multi-level tree for Tr > 16 (one search): level kernels write the partial planes of
 // every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).
 cudaError_t levels_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
-                          cudaStream_t stream);
+                          cudaStream_t stream, const LevelPlan& plan = LevelPlan{});
+
+// A fully planned search for exec_queue: the request, its drift plan and its scratch.
+struct ExecSearch {
+  const float* input;
+  long long row_stride;
+  int T, Tr, N;
+  int dmin, dmax, window_size;
+  double snr_threshold;
+  int elem;  // kElemF32, or the 16-bit storage of the precision form
+  LevelPlan level_plan;
+  int cand_cap;
+  // scratch (carve() lays it out from one base pointer)
+  float* top;
+  float* colsum;
+  SelectState* sel;
+  MomentPartial* partials;
+  double* var;
+  SearchHeader* hdr;
+  Candidate* cands;
+  void* norm16;
+  float* top16;
+  int* tiles;
+  int* tile_count;
+  double* norm_moments;
+  unsigned* norm_ticket;
+  static size_t scratch_bytes(int Tr, int N, int cand_cap, int n_partials, int elem);
+  void carve(char* base, int n_partials);
+};
+
+// Callbacks of exec_queue: the shared-memory budget of each tree launch (autotuning) and
+// points at which the caller may record events.
+struct ExecHooks {
+  void* ctx = nullptr;
+  int (*budget_kb)(void* ctx, const TreeBatch& tb, int R, int elem) = [](void*, const TreeBatch&, int, int) {
+    return 0;
+  };
+  // The level split of a search with more than 16 rows (may time alternatives first).
+  LevelPlan (*level_plan)(void* ctx, const ExecSearch& s, float* lvl_a, float* lvl_b, cudaStream_t st) = nullptr;
+  void (*after_stats)(void* ctx, cudaStream_t s) = nullptr;
+  void (*after_tree)(void* ctx, cudaStream_t s) = nullptr;
+};
+
+// Queues every kernel of n searches (any mix) on `stream`; no synchronisation.
+// lvl_a / lvl_b: level buffers of at least Tr*N floats for every search with Tr > 16.
+cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
+                       const ExecHooks& hooks);
 
 // Decodes a resolved candidate: returns false if the recovered path sum does not equal the
 // stored top sum (a consistency failure).  Paths are numbered (db - dmin) * Tr + off.

@@ -63,13 +63,26 @@ __global__ void emit_kernel(const float* __restrict__ src, long long src_stride,
 
 cudaError_t levels_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
-                          cudaStream_t stream) {
-  int sizes[16];
+                          cudaStream_t stream, const LevelPlan& plan) {
+  int sizes[12];
   int nlev = 0;
-  for (int tp = Tr; tp > 16;) {
-    const int M = (tp / 4 >= 16) ? 4 : 2;
-    sizes[nlev++] = M;
-    tp /= M;
+  int final_rows = 16;
+  if (plan.n > 0) {
+    int prod = plan.final_rows;
+    for (int l = 0; l < plan.n; ++l) {
+      if (plan.m[l] != 2 && plan.m[l] != 4) return cudaErrorInvalidValue;
+      sizes[nlev++] = plan.m[l];
+      prod *= plan.m[l];
+    }
+    final_rows = plan.final_rows;
+    if (prod != Tr || (final_rows != 2 && final_rows != 4 && final_rows != 8 && final_rows != 16))
+      return cudaErrorInvalidValue;
+  } else {
+    for (int tp = Tr; tp > 16;) {
+      const int M = (tp / 4 >= 16) ? 4 : 2;
+      sizes[nlev++] = M;
+      tp /= M;
+    }
   }
   for (int db = dmin; db <= dmax; ++db) {
     const float* src = input;
@@ -97,7 +110,7 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     tp = TreeGroup{};
     tp.rows = src;
     tp.row_stride = N;
-    tp.job_row_stride = 16ll * N;
+    tp.job_row_stride = (long long)final_rows * N;
     tp.N = N;
     tp.d_first = (int)(dscale * db);
     tp.d_step = 1;
@@ -105,10 +118,10 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     tp.db_first = db;
     tp.db_step = 0;
     tp.off_base = 0;
-    tp.off_step = 16;
+    tp.off_step = final_rows;
     tp.elig_T1 = Tr - 1;
     tp.top = top;
-    cudaError_t err = tree_max_batch(tb, 16, num_sms, stream);
+    cudaError_t err = tree_max_batch(tb, final_rows, num_sms, stream);
     if (err != cudaSuccess) return err;
   }
   return cudaGetLastError();
