@@ -52,12 +52,13 @@ def test_mixed_batch_equals_each_request_alone(torch_cuda):
     from seticore_b200 import SearchPool
     reqs = _mixed_requests(torch_cuda)
     alone = [_alone(r) for r in reqs]
-    pool = SearchPool(scratch_budget_bytes=64 << 20)  # small budget: several admitted sub-batches
+    total = sum(SearchPool.scratch_bytes(r) for r in reqs)
+    pool = SearchPool(scratch_budget_bytes=total // 5)  # a small budget: several admitted sub-batches
     for call in range(3):
         got = pool.search_raw(reqs)
         assert [_key(h) for h in got] == alone, f"call {call}"
     st = pool.stats()
-    assert st.calls == 3 and st.sub_batches >= 6
+    assert st.calls == 3 and st.sub_batches >= 3 * 5
     assert st.graph_captures >= 1 and st.graph_replays >= 1
     assert st.tuned_launches >= 1
     pool.close()
