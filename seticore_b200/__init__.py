@@ -5,6 +5,7 @@ The search runs in hand-written CUDA kernels (seticore_b200/csrc) behind a C ABI
 """
 from ._capi import NO_BEAM, DedopplerError  # noqa: F401
 from .pool import SearchPool, SearchRequest  # noqa: F401
+from .serving import SearchServer, run_load  # noqa: F401
 from .dedoppler import (  # noqa: F401
     DedopplerHit,
     Dedopplerer,
