@@ -167,6 +167,195 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def _hit_keys(res):
+    return [[(h.index, h.drift_steps, h.power) for h in hs] for hs in res]
+
+
+def _uneven_requests(torch, n, precision_t16="fp32", seed=4000):
+    """The uneven mix on the device: T in {16..256}, N in {2^16..2^20}, max_drift U(1, 10)."""
+    from seticore_b200 import SearchRequest
+    from seticore_b200.synthetic import config_uneven, make_filterbank_torch
+    specs = config_uneven(n, base_seed=seed)
+    reqs = []
+    for i, sp in enumerate(specs):
+        x = make_filterbank_torch(sp)
+        reqs.append(SearchRequest(x, sp.num_timesteps, sp.foff_mhz, sp.tsamp, sp.max_drift, sp.min_drift,
+                                  sp.snr_threshold, beam=-1, coarse_channel=i,
+                                  precision=precision_t16 if sp.rounded_timesteps <= 16 else "fp32"))
+    torch.cuda.synchronize()
+    return specs, reqs
+
+
+def _with_precision(reqs, prec):
+    import dataclasses
+    return [dataclasses.replace(r, precision=prec if r.input.shape[0] <= 16 else "fp32") for r in reqs]
+
+
+def _time_pool(torch, pool, reqs, steps, warmup, stream):
+    for _ in range(max(3, warmup)):
+        pool.search_raw(reqs, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        res = pool.search_raw(reqs, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, res
+
+
+def run_uneven(args, world, rank, local):
+    """Batched uneven searches through the pool (sc_dd_pool): autotuned on the first call,
+    captured as CUDA graphs on the second, replayed afterwards; FP32, and BF16 storage for
+    the searches of 16 timesteps (the 16-bit forms cover up to 16 rounded timesteps)."""
+    import torch
+    from seticore_b200 import SearchPool
+    n = args.count or 512
+    specs, reqs = _uneven_requests(torch, n, seed=4000 + 1000 * rank)
+    samples = sum(r.input.shape[0] * r.input.shape[1] for r in reqs)
+    stream = torch.cuda.current_stream()
+    pool = SearchPool(scratch_budget_bytes=16 << 30)
+    barrier(world)
+    clocks = Clocks(local)
+    clocks.start()
+    ms, res32 = _time_pool(torch, pool, reqs, args.steps, args.warmup, stream)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms, world)
+    st = pool.stats()
+    calls = max(1, st.calls)
+    out = {"metric": "dedoppler Gsamples/s (FP32, 512 uneven searches)", "value": world * samples / (ms / 1e3) / 1e9,
+           "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"uneven: {n} searches, T in {{16,32,64,128,256}}, N in {{2^16,2^17,2^18,2^20}}, "
+                                  "max_drift U(1,10) Hz/s, 0-6 tones SNR 12-80", "samples_per_step": samples,
+                      "input_bytes": samples * 4, "l2": "inputs larger than L2; no flush"},
+           "pool": {"sub_batches_per_call": st.sub_batches / calls, "graph_captures": st.graph_captures,
+                    "graph_replays": st.graph_replays, "tuned_launches": st.tuned_launches},
+           "clocks": clk, "hits_per_step": sum(len(h) for h in res32)}
+    keys32 = _hit_keys(res32)
+    # The searches of 16 timesteps alone, FP32 against BF16 / FP16 storage (identical hits required).
+    t16 = [r for r in reqs if r.input.shape[0] <= 16]
+    sub = {}
+    if t16:
+        s16 = sum(r.input.shape[0] * r.input.shape[1] for r in t16)
+        for prec in ["fp32", "bf16", "fp16"]:
+            rq = _with_precision(t16, prec)
+            p = SearchPool(scratch_budget_bytes=16 << 30)
+            m, r = _time_pool(torch, p, rq, args.steps, args.warmup, stream)
+            m = max_over_ranks(m, world)
+            sub[prec] = {"value": world * s16 / (m / 1e3) / 1e9, "ms_per_step": m}
+            if prec == "fp32":
+                k32 = _hit_keys(r)
+            else:
+                sub[prec]["hits_identical_to_fp32"] = _hit_keys(r) == k32
+            p.close()
+        sub["searches"] = len(t16)
+        sub["samples_per_step"] = s16
+    out["t16_subset"] = sub
+    # The whole mix with BF16 storage where it applies.
+    rq = _with_precision(reqs, "bf16")
+    p = SearchPool(scratch_budget_bytes=16 << 30)
+    m, r = _time_pool(torch, p, rq, args.steps, args.warmup, stream)
+    m = max_over_ranks(m, world)
+    out["bf16_mix"] = {"value": world * samples / (m / 1e3) / 1e9, "ms_per_step": m,
+                       "hits_identical_to_fp32": _hit_keys(r) == keys32}
+    p.close()
+    pool.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_serve(args, world, rank, local):
+    """Continuous batching (seticore_b200.serving): Poisson arrivals of searches drawn from
+    the uneven mix, admitted by a 120 GB HBM budget, inputs resident on the device.
+    Capacity is measured first with every request submitted at once; then arrivals are
+    offered at 0.5, 0.8, 1.0 and 1.2 x capacity.  Latency is arrival to result (wall clock)."""
+    import torch
+    from seticore_b200 import SearchPool, SearchServer, run_load
+    n_inputs = args.count or 128
+    specs, reqs = _uneven_requests(torch, n_inputs, seed=5000 + 1000 * rank)
+    stream = torch.cuda.current_stream()
+    ref = SearchPool(scratch_budget_bytes=16 << 30)
+    ref_keys = _hit_keys(ref.search_raw(reqs, stream=stream))
+    ref.close()
+    budget = 120 << 30
+    out = {"metric": "serving p50/p99 latency and Gsamples/s (uneven mix)", "unit": "s", "n_gpus": world,
+           "data": "synthetic", "higher_is_better": False,
+           "config": {"workload": f"serve: {n_inputs} resident inputs from the uneven mix, Poisson arrivals, "
+                                  "120 GB HBM budget, 2 workers", "budget_bytes": budget}, "forms": {}}
+    for form in ["fp32", "bf16"]:
+        base = reqs if form == "fp32" else _with_precision(reqs, "bf16")
+        server = SearchServer(hbm_budget_bytes=budget, workers=2, max_batch=64)
+        # warm-up (autotuning, graphs) and identical-hits check
+        got = [f.result() for f in [server.submit(r) for r in base]]
+        identical = _hit_keys([g[0] for g in got]) == ref_keys
+        t0 = time.perf_counter()
+        n_cap = 2 * n_inputs
+        futs = [server.submit(base[i % n_inputs]) for i in range(n_cap)]
+        for f in futs:
+            f.result()
+        cap_s = time.perf_counter() - t0
+        cap_rps = n_cap / cap_s
+        samples = sum(base[i % n_inputs].input.shape[0] * base[i % n_inputs].input.shape[1] for i in range(n_cap))
+        points = []
+        for load in [0.5, 0.8, 1.0, 1.2]:
+            rate = load * cap_rps
+            n_req = int(min(4 * n_inputs, max(64, rate * args.serve_seconds)))
+            _, lat, wall, smp = run_load(lambda i: base[i % n_inputs], n_req, rate, server, seed=int(load * 100))
+            points.append({"offered_load": load, "rate_per_s": rate, "requests": n_req,
+                           "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                           "gsamples_per_s": smp / wall / 1e9})
+        st = dict(server.stats)
+        server.close()
+        out["forms"][form] = {"capacity_requests_per_s": cap_rps, "capacity_gsamples_per_s": samples / cap_s / 1e9,
+                              "hits_identical_to_fp32": identical, "points": points, "server": st}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_beams(args, world, rank, local):
+    """Beamformed-style case: 64 beams x 256 timesteps x 131072 channels (foff 3.81 Hz,
+    tsamp 0.268 s, max_drift 10 Hz/s), one batched call; more than 16 rows, so the
+    level path runs."""
+    import torch
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import config_beams, make_filterbank_torch
+    n = args.count or 64
+    specs = config_beams(n, base_seed=3000 + 1000 * rank)
+    sp = specs[0]
+    data = torch.empty((n, sp.rounded_timesteps, sp.num_channels), dtype=torch.float32, device="cuda")
+    for i, s in enumerate(specs):
+        make_filterbank_torch(s, out=data[i])
+    torch.cuda.synchronize()
+    dd = Dedopplerer(sp.num_timesteps, sp.num_channels, sp.foff_mhz, sp.tsamp)
+    stream = torch.cuda.current_stream()
+    inputs = [data[i] for i in range(n)]
+    for _ in range(max(3, args.warmup)):
+        res = dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold, stream=stream)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        res = dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    samples = n * sp.rounded_timesteps * sp.num_channels
+    out = {"metric": "dedoppler Gsamples/s (FP32, 64 beams x 256 x 131072)", "value": world * samples / (ms / 1e3) / 1e9,
+           "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"beams: {n} x 256 x 131072, foff 3.81 Hz, tsamp 0.268 s, max_drift 10 Hz/s",
+                      "drift_blocks": sp.num_drift_blocks(), "input_bytes": samples * 4},
+           "clocks": clk, "hits_per_step": sum(len(h) for h in res)}
+    dd.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -178,8 +367,18 @@ def main():
     ap.add_argument("--fp32-only", action="store_true", help="skip the BF16/FP16 precision-form lines")
     ap.add_argument("--coarse", type=int, default=N_COARSE,
                     help="coarse channels per node (64; fewer only for small profiling captures)")
+    ap.add_argument("--workload", default="node", choices=["node", "uneven", "serve", "beams"],
+                    help="node (the headline line); uneven, serve and beams print their own lines")
+    ap.add_argument("--count", type=int, default=0, help="searches of the uneven / serve / beams workloads")
+    ap.add_argument("--serve-seconds", type=float, default=8.0, help="offered-load duration per serving point")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.impl == "ours" and args.workload != "node":
+        {"uneven": run_uneven, "serve": run_serve, "beams": run_beams}[args.workload](args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:
