@@ -142,6 +142,23 @@ const char* sc_dd_last_error(void);
 /* Library version string. */
 const char* sc_dd_version(void);
 
+/* The device half of H5Reader::loadCoarseChannel (h5_reader.cpp:190-209) for `count`
+ * coarse channels laid out item_stride floats apart, each [rounded_timesteps][row_stride]:
+ * rows num_timesteps .. rounded_timesteps-1 become zero and, if has_dc_spike, column
+ * num_channels/2 of every loaded row becomes (left + right) / 2.  Stream-ordered, one
+ * launch, no synchronisation.  The reference does both on the host after the read. */
+int sc_dd_prepare_coarse_channels(float* dev_base, int count, long long item_stride, long long row_stride,
+                                  int num_timesteps, int rounded_timesteps, int num_channels,
+                                  int has_dc_spike, void* stream);
+
+/* The filterbank slices stored with hits in .hits files (hit_file_writer.cpp:81-96):
+ * for k < count, rows [0, num_timesteps) and columns [dev_ranges[2k], dev_ranges[2k+1])
+ * of dev_input go, row-major, to dev_out + dev_offsets[k].  All arrays are device memory;
+ * one launch, no synchronisation.  The reference copies each slice on the host. */
+int sc_dd_gather_columns(const float* dev_input, long long row_stride, int num_timesteps, int num_channels,
+                         const int* dev_ranges, const long long* dev_offsets, int count, float* dev_out,
+                         void* stream);
+
 /* ---- Heterogeneous batches: many searches of different shapes at once ---- */
 
 /* One search request: its input, the shape sc_dd_create would take, and the arguments

@@ -36,6 +36,15 @@ int cuda_fail(cudaError_t err, const char* what) {
   return fail(SC_DD_ECUDA, std::string(what) + ": " + cudaGetErrorString(err));
 }
 
+}  // namespace
+
+namespace scb {
+// Sets the calling thread's sc_dd_last_error message (for the other ABI translation units).
+int api_fail(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace scb
+
+namespace {
+
 constexpr int kHostCands = 256;  // candidates per search fetched with the headers
 
 int round_up_pow2(int n) {  // util.cpp:16-22
@@ -249,32 +258,6 @@ int ensure_inc(sc_dd* d, int n) {
     return cuda_fail(e, "incoherent staging allocation");
   d->inc_cap = cap;
   return SC_DD_OK;
-}
-
-scb::SearchDesc make_desc(sc_dd* d, int slot, const float* input, long long row_stride, const DriftPlan& p,
-                          double snr_threshold) {
-  scb::SearchDesc s{};
-  const size_t N = d->N;
-  s.input = input;
-  s.row_stride = row_stride;
-  s.Tr = d->Tr;
-  s.N = d->N;
-  s.dmin = p.dmin;
-  s.dmax = p.dmax;
-  s.window_size = p.window_size;
-  s.first = (int)std::ceil(0.05 * d->N);  // dedoppler.cu:327
-  s.mid = d->N / 2;                        // dedoppler.cu:291
-  s.last = (int)std::floor(0.95 * d->N);  // dedoppler.cu:328
-  s.snr_threshold = snr_threshold;
-  s.top = d->top + N * slot;
-  s.colsum = d->colsum + N * slot;
-  s.sel = d->sel + slot;
-  s.partials = d->partials + (size_t)d->n_partials * slot;
-  s.var = d->var + (size_t)2 * scb::kVarChunks * slot;
-  s.hdr = d->hdrs + slot;
-  s.cands = d->cands + (size_t)d->cand_cap * slot;
-  s.cand_cap = d->cand_cap;
-  return s;
 }
 
 // Queues n <= kMaxBatch searches into slots 0..n-1.

@@ -39,9 +39,35 @@ class FilterbankMetadata:
     has_dc_spike: bool = False
     source_name: str = ""
     source_names: List[str] = field(default_factory=list)
+    ras: List[float] = field(default_factory=list)   # hours, per coherent beam
+    decs: List[float] = field(default_factory=list)  # degrees, per coherent beam
+    tstart: float = 0.0  # MJD
+    src_raj: float = 0.0  # hours
+    src_dej: float = 0.0  # degrees
+    telescope_id: int = 0
 
     def isCoherentBeam(self, beam: int) -> bool:  # filterbank_metadata.cpp:116-118
         return 0 <= beam < len(self.source_names)
+
+    def getBeamSourceName(self, beam: int) -> str:  # filterbank_metadata.cpp:95-100
+        return self.source_names[beam] if self.isCoherentBeam(beam) else self.source_name
+
+    def getBeamRA(self, beam: int) -> float:  # filterbank_metadata.cpp:102-107
+        return self.ras[beam] if self.isCoherentBeam(beam) else self.src_raj
+
+    def getBeamDec(self, beam: int) -> float:  # filterbank_metadata.cpp:109-114
+        return self.decs[beam] if self.isCoherentBeam(beam) else self.src_dej
+
+    def getSubsetMetadata(self, beam: int, band: int, num_bands: int) -> "FilterbankMetadata":
+        """The metadata of one band of one beam (filterbank_metadata.cpp:22-50)."""
+        import dataclasses
+        n = self.num_channels // num_bands
+        assert n > 0
+        return dataclasses.replace(
+            self, source_name=self.getBeamSourceName(beam), source_names=list(self.source_names),
+            ras=list(self.ras), decs=list(self.decs), num_channels=n,
+            num_coarse_channels=self.num_coarse_channels // num_bands, fch1=self.fch1 + self.foff * n * band,
+            src_raj=self.getBeamRA(beam), src_dej=self.getBeamDec(beam))
 
 
 @dataclass
@@ -168,6 +194,44 @@ def _stream_handle(stream):
     return ctypes.c_void_p(s.cuda_stream)
 
 
+def prepare_coarse_channels(buffers, num_timesteps: int, has_dc_spike: bool, stream=None) -> None:
+    """The device half of loading coarse channels (h5_reader.cpp:190-209), one launch for a
+    [count][rounded T][N] CUDA tensor (or one [rounded T][N] tensor): zeroes the rows past
+    num_timesteps and, with has_dc_spike, replaces the middle column of each loaded row by
+    the mean of its neighbours (sc_dd_prepare_coarse_channels)."""
+    t = buffers if buffers.dim() == 3 else buffers.unsqueeze(0)
+    if not t.is_cuda or t.dtype.itemsize != 4 or t.stride(2) != 1:
+        raise TypeError("prepare_coarse_channels needs a float32 CUDA tensor with unit channel stride")
+    check(lib().sc_dd_prepare_coarse_channels(ctypes.c_void_p(t.data_ptr()), t.shape[0], t.stride(0), t.stride(1),
+                                              num_timesteps, t.shape[1], t.shape[2], int(has_dc_spike),
+                                              _stream_handle(stream)))
+
+
+def gather_hit_slices(input, num_timesteps: int, num_channels: int, bounds, stream=None):
+    """Rows [0, num_timesteps) and columns [begin, end) of a CUDA tensor for each (begin,
+    end) in bounds, gathered by one kernel launch (sc_dd_gather_columns) and copied to the
+    host once.  Returns a list of float32 numpy arrays."""
+    import numpy as np
+    import torch
+    n = len(bounds)
+    if n == 0:
+        return []
+    widths = [max(0, e - b) for b, e in bounds]
+    offs = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum([num_timesteps * w for w in widths], out=offs[1:])
+    dev = input.device
+    ranges = torch.tensor([v for b, e in bounds for v in (b, max(b, e))], dtype=torch.int32, device=dev)
+    offsets = torch.from_numpy(offs[:-1].copy()).to(dev)
+    out = torch.empty(max(1, int(offs[-1])), dtype=torch.float32, device=dev)
+    check(lib().sc_dd_gather_columns(ctypes.c_void_p(input.data_ptr()), input.stride(0), num_timesteps, num_channels,
+                                     ctypes.c_void_p(ranges.data_ptr()), ctypes.c_void_p(offsets.data_ptr()), n,
+                                     ctypes.c_void_p(out.data_ptr()), _stream_handle(stream)))
+    if stream is not None:
+        stream.synchronize()
+    host = out.cpu().numpy()
+    return [host[offs[k]:offs[k + 1]].reshape(num_timesteps, widths[k]) for k in range(n)]
+
+
 class Dedopplerer:
     """The dedoppler search engine (dedoppler.h:15-79) on one CUDA device."""
 
@@ -259,9 +323,14 @@ class Dedopplerer:
         meta = metadata or FilterbankMetadata(foff=self.foff, tsamp=self.tsamp,
                                               coarse_channel_size=self.num_channels)
         res = self.search_batch_raw(inputs, beams, coarse_channels, max_drift, min_drift, snr_threshold, stream)
-        return [[DedopplerHit.make(meta, h.index, h.drift_steps, h.drift_rate, h.snr, b, c, self.num_timesteps,
-                                   h.power) for h in hits]
-                for hits, b, c in zip(res, beams, coarse_channels)]
+        out = [[DedopplerHit.make(meta, h.index, h.drift_steps, h.drift_rate, h.snr, b, c, self.num_timesteps,
+                                  h.power) for h in hits]
+               for hits, b, c in zip(res, beams, coarse_channels)]
+        if self.print_hits:
+            for hits in out:
+                for hit in hits:
+                    print("hit: " + hit.toString())
+        return out
 
     def search(self, input, metadata: Optional[FilterbankMetadata], beam: int, coarse_channel: int,
                max_drift: float, min_drift: float, snr_threshold: float,
