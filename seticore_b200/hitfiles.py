@@ -28,11 +28,10 @@ slot allocation and agree with the generated accessors (hit.capnp.h):
 allocates them in HitFileWriter::recordHit -- root pointer, Hit, Signal, Filterbank, source
 name, data -- in one segment, so the bytes match the reference writer's for messages that fit
 its first segment (1024 words).  The filterbank slice is gathered on the GPU
-(sc_dd_gather_hit_slices) when the input is a device tensor.
+(sc_dd_gather_columns) when the input is a device tensor.
 """
 import os
 import struct
-from dataclasses import dataclass, field
 from typing import List, Optional
 
 import numpy as np
@@ -91,34 +90,68 @@ def _fill(seg: _Segment, at_word: int, data_words: int, fields, values: dict):
         struct.pack_into(_FMT[kind], seg.words, base + off, float(v) if kind in "df" else int(v))
 
 
+def _put_signal(seg: _Segment, ptr_word: int, signal: dict, layout):
+    sdw, spw = layout["Signal"]
+    s = seg.alloc(sdw + spw)
+    seg.point_struct(ptr_word, s, sdw, spw)
+    _fill(seg, s, sdw, SIGNAL_FIELDS, signal)
+
+
+def _put_filterbank(seg: _Segment, ptr_word: int, filterbank: dict, layout):
+    fdw, fpw = layout["Filterbank"]
+    f = seg.alloc(fdw + fpw)
+    seg.point_struct(ptr_word, f, fdw, fpw)
+    name = filterbank.get("sourceName", "").encode() + b"\0"
+    t = seg.alloc((len(name) + 7) // 8)
+    seg.point_list(f + fdw + 0, t, 2, len(name))
+    seg.words[8 * t: 8 * t + len(name)] = name
+    _fill(seg, f, fdw, FILTERBANK_FIELDS, filterbank)
+    data = np.ascontiguousarray(filterbank.get("data", np.zeros(0, np.float32)), dtype="<f4").ravel()
+    d = seg.alloc((data.size + 1) // 2)
+    seg.point_list(f + fdw + 1, d, 4, data.size)
+    seg.words[8 * d: 8 * d + 4 * data.size] = data.tobytes()
+
+
+def _frame(seg: _Segment) -> bytes:
+    return struct.pack("<II", 0, len(seg.words) // 8) + bytes(seg.words)
+
+
 def encode_hit(signal: Optional[dict], filterbank: Optional[dict], layout=LAYOUT) -> bytes:
     """One Hit message (unpacked stream framing).  `filterbank["data"]` is a float32 array
-    of numTimesteps x numChannels values (row-major) and `filterbank["sourceName"]` a str."""
+    of numTimesteps x numChannels values (row-major) and `filterbank["sourceName"]` a str.
+    Allocation order of HitFileWriter::recordHit: Hit, Signal, Filterbank, name, data."""
     seg = _Segment()
     root = seg.alloc(1)
     hdw, hpw = layout["Hit"]
     hit = seg.alloc(hdw + hpw)
     seg.point_struct(root, hit, hdw, hpw)
     if signal is not None:
-        sdw, spw = layout["Signal"]
-        s = seg.alloc(sdw + spw)
-        seg.point_struct(hit + hdw + 0, s, sdw, spw)
-        _fill(seg, s, sdw, SIGNAL_FIELDS, signal)
+        _put_signal(seg, hit + hdw + 0, signal, layout)
     if filterbank is not None:
-        fdw, fpw = layout["Filterbank"]
-        f = seg.alloc(fdw + fpw)
-        seg.point_struct(hit + hdw + 1, f, fdw, fpw)
-        name = filterbank.get("sourceName", "").encode() + b"\0"
-        t = seg.alloc((len(name) + 7) // 8)
-        seg.point_list(f + fdw + 0, t, 2, len(name))
-        seg.words[8 * t: 8 * t + len(name)] = name
-        _fill(seg, f, fdw, FILTERBANK_FIELDS, filterbank)
-        data = np.ascontiguousarray(filterbank.get("data", np.zeros(0, np.float32)), dtype="<f4").ravel()
-        d = seg.alloc((data.size + 1) // 2)
-        seg.point_list(f + fdw + 1, d, 4, data.size)
-        seg.words[8 * d: 8 * d + 4 * data.size] = data.tobytes()
-    n = len(seg.words) // 8
-    return struct.pack("<II", 0, n) + bytes(seg.words)
+        _put_filterbank(seg, hit + hdw + 1, filterbank, layout)
+    return _frame(seg)
+
+
+def encode_event(hits, layout=LAYOUT) -> bytes:
+    """One Event message (hit.capnp: Event { hits @0 :List(Hit) }) for a list of
+    (signal or None, filterbank) pairs.  Allocation order of EventFileWriter::write
+    (event_file_writer.cpp:36-70): Event, the composite list of Hits, then per hit its
+    Filterbank (name, data) followed by its Signal."""
+    seg = _Segment()
+    root = seg.alloc(1)
+    event = seg.alloc(1)  # Event: 0 data words, 1 pointer
+    seg.point_struct(root, event, 0, 1)
+    hdw, hpw = layout["Hit"]
+    n = len(hits)
+    tag = seg.alloc(1 + n * (hdw + hpw))
+    seg.point_list(event, tag, 7, n * (hdw + hpw))
+    seg.put_ptr(tag, _struct_ptr(n, hdw, hpw))  # composite-list tag: element count and size
+    for i, (signal, filterbank) in enumerate(hits):
+        h = tag + 1 + i * (hdw + hpw)
+        _put_filterbank(seg, h + hdw + 1, filterbank, layout)
+        if signal is not None:
+            _put_signal(seg, h + hdw + 0, signal, layout)
+    return _frame(seg)
 
 
 # ---------------------------------------------------------------- decoder
@@ -155,11 +188,16 @@ def _get(seg, at, dw, fields):
     return out
 
 
-def decode_hit(seg: bytes) -> dict:
-    """The Signal and Filterbank of one single-segment Hit message (fields missing from an
-    older, smaller layout read as zero, as capnp's schema evolution defines)."""
-    r = _read_struct(seg, 0)
+def decode_hit(seg: bytes, ptr_word: int = 0) -> dict:
+    """The Signal and Filterbank of a Hit whose struct pointer is at ptr_word (0: the root
+    of a single-segment Hit message).  Fields missing from an older, smaller layout read as
+    zero, as capnp's schema evolution defines."""
+    r = _read_struct(seg, ptr_word)
     hit, hdw, hpw = r
+    return _decode_hit_at(seg, hit, hdw, hpw)
+
+
+def _decode_hit_at(seg: bytes, hit: int, hdw: int, hpw: int) -> dict:
     out = {"signal": None, "filterbank": None}
     if hpw > 0:
         s = _read_struct(seg, hit + hdw + 0)
@@ -179,6 +217,20 @@ def decode_hit(seg: bytes) -> dict:
                           if d else np.zeros(0, np.float32))
             out["filterbank"] = fb
     return out
+
+
+def decode_event(seg: bytes) -> List[dict]:
+    """The Hits of one single-segment Event message."""
+    ev = _read_struct(seg, 0)
+    lst = _read_list(seg, ev[0] + ev[1])
+    if lst is None:
+        return []
+    at, size_code, _ = lst
+    if size_code != 7:
+        raise ValueError("Event.hits is not a composite list")
+    tag = struct.unpack_from("<Q", seg, 8 * at)[0]
+    n, dw, pw = (tag >> 2) & 0x3FFFFFFF, (tag >> 32) & 0xFFFF, (tag >> 48) & 0xFFFF
+    return [_decode_hit_at(seg, at + 1 + i * (dw + pw), dw, pw) for i in range(n)]
 
 
 def split_messages(blob: bytes):
@@ -212,18 +264,22 @@ def _slice_bounds(hit, coarse_channel_size: int):
     return begin, end
 
 
-def gather_slices(hits, input, metadata) -> List[np.ndarray]:
-    """The [num_timesteps][end - begin] slice of `input` for each hit.  A CUDA tensor input
-    is gathered by one kernel launch (sc_dd_gather_hit_slices) and copied back once; a
-    host array is sliced directly."""
+def gather_ranges(input, metadata, bounds) -> List[np.ndarray]:
+    """The [num_timesteps][end - begin] slice of `input` for each (begin, end).  A CUDA
+    tensor input is gathered by one kernel launch (sc_dd_gather_columns) and copied back
+    once; a host array is sliced directly."""
     T = int(metadata.num_timesteps)
     N = int(metadata.coarse_channel_size)
-    bounds = [_slice_bounds(h, N) for h in hits]
     if hasattr(input, "is_cuda") and input.is_cuda:
         from .dedoppler import gather_hit_slices
         return gather_hit_slices(input, T, N, bounds)
     x = np.asarray(input, dtype=np.float32).reshape(-1, N)
     return [np.ascontiguousarray(x[:T, b:e]) for b, e in bounds]
+
+
+def gather_slices(hits, input, metadata) -> List[np.ndarray]:
+    """The slice a .hits file stores with each hit (gather_ranges of _slice_bounds)."""
+    return gather_ranges(input, metadata, [_slice_bounds(h, int(metadata.coarse_channel_size)) for h in hits])
 
 
 class HitRecorder:

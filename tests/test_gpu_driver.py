@@ -161,3 +161,45 @@ def test_multibeam_band_search_in_place(torch_cuda):
         [_key(h) + (np.float32(h.incoherent_power),) for h in want]
     assert {h.beam for h in got} == {0, 1, 2}
     assert all(h.incoherent_power > 0 for h in got)
+
+
+def _tone(x, c0, steps_per_row, amp):
+    for t in range(x.shape[0]):
+        c = c0 + int(round(t * steps_per_row))
+        if 0 <= c < x.shape[1]:
+            x[t, c] += amp
+
+
+def test_find_events_on_a_synthetic_cadence(torch_cuda, tmp_path):
+    """ABACAD: a drifting tone in the three "on" files only is one event; a drifting tone in
+    all six files (at lower channels) is not."""
+    from seticore_b200.events import findEvents
+    from seticore_b200.hitfiles import decode_event, split_messages
+    from seticore_b200.run_dedoppler import ArrayFilterbankFile
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    N, T = 65536, 16
+    files = []
+    rate = 8.0 / 15.0  # channels per timestep
+    for i in range(6):
+        spec = SearchSpec(T, N, seed=3000 + i, n_tones=0)
+        x = make_filterbank_numpy(spec)[:T]
+        sigma = np.std(np.sort(x.sum(axis=0, dtype=np.float64))[int(np.ceil(0.05 * N)):int(0.95 * N) + 1])
+        tstart = i * 300.0
+        t_off = tstart / spec.tsamp
+        _tone(x, 10000 + int(round(rate * t_off)), rate, 40 * sigma / T)  # in every file
+        if i % 2 == 0:
+            _tone(x, 40000 + int(round(rate * t_off)), rate, 40 * sigma / T)
+        files.append(ArrayFilterbankFile(x, coarse_channel_size=N, telescope_id=6, foff=spec.foff_mhz,
+                                         tsamp=spec.tsamp, tstart=tstart / 86400.0 * 86400.0, fch1=8000.0,
+                                         source_name="TGT" if i % 2 == 0 else f"OFF{i}"))
+    out = str(tmp_path / "c.events")
+    events = findEvents(files, out, 2.0, 10.0, 10.0, verbose=False)
+    assert len(events) == 1
+    ev = events[0]
+    assert [h is None for h in ev] == [False, True, False, True, False, True]
+    assert abs(ev[0].index - 40000) <= 2
+    msgs = [decode_event(seg) for _, seg in split_messages(open(out, "rb").read())]
+    assert len(msgs) == 1 and len(msgs[0]) == 6
+    assert [m["signal"] is None for m in msgs[0]] == [False, True, False, True, False, True]
+    assert [m["filterbank"]["sourceName"] for m in msgs[0]] == ["TGT", "OFF1", "TGT", "OFF3", "TGT", "OFF5"]
+    assert all(m["filterbank"]["data"].size == T * m["filterbank"]["numChannels"] for m in msgs[0])
