@@ -29,6 +29,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from seticore_b200.replicas import barrier, max_over_ranks  # noqa: E402
+
 N_COARSE = 64
 T = 16
 N = 1 << 20
@@ -36,9 +38,9 @@ MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum) from the ncu capture summarised in profiles/tree_max_kernel_node.md;
-# a launch covering k coarse channels moves k times this.
-TREE_DRAM_BYTES = 71950848
+# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.34 MB +
+# 15.31 MB); a launch covering k coarse channels moves k times this.
+TREE_DRAM_BYTES = 75163904
 
 
 def dist_setup():
@@ -55,22 +57,6 @@ def dist_setup():
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return world, rank, local
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
 
 
 class Clocks:

@@ -4,7 +4,7 @@
 // (dedoppler.cu:186-320), its Taylor tree (taylor.cu:116-156 schedule, recursion
 // taylor.h:30-86), findTopPathSums (dedoppler.cu:32-55), sumColumns (dedoppler.cu:63-72)
 // and addIncoherentPower (dedoppler.cu:139-176).  It is used only by the test suite,
-// by __graft_entry__.smoke() as the checker, and by bench.py's CPU-baseline leg.
+// by __graft_entry__.smoke() to check its result, and by bench.py's CPU-baseline leg.
 // The product path (seticore_b200/) never links, loads or calls it.
 //
 // Built two ways (oracle/Makefile):

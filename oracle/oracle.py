@@ -1,6 +1,6 @@
 """Python bindings of the oracles.  TEST INFRASTRUCTURE ONLY.
 
-Only tests/, __graft_entry__.smoke() (as the checker) and bench.py's CPU-baseline /
+Only tests/, __graft_entry__.smoke() (to check its result) and bench.py's CPU-baseline /
 reference legs use this module; the product (seticore_b200/) never imports it.
 
   Oracle("port")       -- oracle/_build/liboracle.so: CPU restatement of the reference

@@ -190,10 +190,10 @@ def test_find_events_on_a_synthetic_cadence(torch_cuda, tmp_path):
         if i % 2 == 0:
             _tone(x, 40000 + int(round(rate * t_off)), rate, 40 * sigma / T)
         files.append(ArrayFilterbankFile(x, coarse_channel_size=N, telescope_id=6, foff=spec.foff_mhz,
-                                         tsamp=spec.tsamp, tstart=tstart / 86400.0 * 86400.0, fch1=8000.0,
+                                         tsamp=spec.tsamp, tstart=tstart, fch1=8000.0,
                                          source_name="TGT" if i % 2 == 0 else f"OFF{i}"))
     out = str(tmp_path / "c.events")
-    events = findEvents(files, out, 2.0, 10.0, 10.0, verbose=False)
+    events = findEvents(files, out, 2.0, 20.0, 20.0, verbose=False)  # above the noise hits (SNR ~10-11)
     assert len(events) == 1
     ev = events[0]
     assert [h is None for h in ev] == [False, True, False, True, False, True]
