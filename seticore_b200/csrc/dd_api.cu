@@ -101,8 +101,8 @@ struct sc_dd {
   double* var = nullptr;
   scb::SearchHeader* hdrs = nullptr;
   scb::Candidate* cands = nullptr;
-  float* scratch_a = nullptr;  // Tr > 16 level buffers (one search at a time)
-  float* scratch_b = nullptr;
+  float* scratch_a = nullptr;  // Tr > 16 level buffers (one search at a time), one allocation
+  float* scratch_b = nullptr;  // = scratch_a + level_buffer_floats(Tr, N)
   void* host = nullptr;  // pinned: slots * (header + kHostCands candidates)
   int* inc_index = nullptr;
   int* inc_steps = nullptr;
@@ -206,8 +206,8 @@ int ensure_prec(sc_dd* d, int slots) {
 void free_all(sc_dd* d) {
   free_slots(d);
   free_prec(d);
-  dfree(d, &d->scratch_a, sizeof(float) * (size_t)d->N * d->Tr);
-  dfree(d, &d->scratch_b, sizeof(float) * (size_t)d->N * d->Tr);
+  d->scratch_b = nullptr;  // inside scratch_a's allocation
+  dfree(d, &d->scratch_a, 2 * sizeof(float) * scb::level_buffer_floats(d->Tr, d->N));
   dfree(d, &d->inc_index, sizeof(int) * d->inc_cap);
   dfree(d, &d->inc_steps, sizeof(int) * d->inc_cap);
   dfree(d, &d->inc_vals, sizeof(float) * d->inc_cap);
@@ -459,9 +459,12 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
   // One slot; candidates for windows of 16 channels or more (grown when a call needs more).
   int rc = ensure_slots(d, 1, std::min(num_channels / 2 + 2, num_channels / 16 + 2));
   if (rc == SC_DD_OK && d->Tr > 16) {
-    if ((e = dalloc(d, &d->scratch_a, sizeof(float) * (size_t)num_channels * d->Tr)) != cudaSuccess ||
-        (e = dalloc(d, &d->scratch_b, sizeof(float) * (size_t)num_channels * d->Tr)) != cudaSuccess)
+    // Both level buffers in one allocation: the emitting level addresses them as one array.
+    if ((e = dalloc(d, &d->scratch_a, 2 * sizeof(float) * scb::level_buffer_floats(d->Tr, num_channels))) !=
+        cudaSuccess)
       rc = fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA, "sc_dd_create: level buffers");
+    else
+      d->scratch_b = d->scratch_a + scb::level_buffer_floats(d->Tr, num_channels);
   }
   for (int i = 0; i < 4 && rc == SC_DD_OK; ++i)
     if ((e = cudaEventCreate(&d->ev[i])) != cudaSuccess) rc = cuda_fail(e, "sc_dd_create: event");

@@ -99,6 +99,11 @@ struct TreeGroup {
   // Optional: only the tiles listed in tile_list[0 .. *tile_count) (device memory).
   const int* tile_list;
   const int* tile_count;
+  // Emitting launches (tree_emit_batch): root offset r of job k at channel c goes to
+  // emit_out[k * emit_job_stride + r * emit_plane_stride + c]; top is unused.
+  float* emit_out;
+  long long emit_job_stride;
+  long long emit_plane_stride;
   int jobs_per_chunk;
   int n_chunks;
   int n_tiles;
@@ -118,8 +123,23 @@ struct TreeBatch {
 cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream, int elem = kElemF32,
                            int smem_budget_kb = 0);
 
+// The same staged tree for 16 rows, writing every root value (all 16 in-block offsets of
+// every channel) to the groups' emit planes instead of folding maxima: the first level of
+// a tree of more than 16 rows.  Values of paths that leave [0, N) are sums with zeros.
+// Every tile is stored whole, so plane rows must hold level_row_length(N) floats.
+cudaError_t tree_emit_batch(TreeBatch& b, int num_sms, cudaStream_t stream, int smem_budget_kb = 0);
+
 // Channels per tree work item (the tile a flag refers to).
 int tree_tile_width();
+
+// Row length of the level planes (N rounded up to whole tiles) and the floats one level
+// buffer holds for a search of Tr rounded timesteps: levels_search needs two such buffers
+// in one allocation (scratch_b = scratch_a + level_buffer_floats).
+inline long long level_row_length(int N) {
+  const long long w = tree_tile_width();
+  return (N + w - 1) / w * w;
+}
+inline size_t level_buffer_floats(int Tr, int N) { return (size_t)Tr * (size_t)level_row_length(N); }
 
 // Precision form (dd_precision.cu), per search of a batch:
 struct PrecisionDesc {
@@ -166,6 +186,7 @@ struct LevelPlan {
 
 // Multi-level tree for Tr > 16 (one search): level kernels write the partial planes of
 // every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).
+// scratch_a / scratch_b: level_buffer_floats(Tr, N) floats each, in one allocation.
 cudaError_t levels_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
                           cudaStream_t stream, const LevelPlan& plan = LevelPlan{});
@@ -212,7 +233,8 @@ struct ExecHooks {
 };
 
 // Queues every kernel of n searches (any mix) on `stream`; no synchronisation.
-// lvl_a / lvl_b: level buffers of at least Tr*N floats for every search with Tr > 16.
+// lvl_a / lvl_b: level buffers of level_buffer_floats(Tr, N) floats for every search with
+// Tr > 16, in one allocation.
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
                        const ExecHooks& hooks);
 

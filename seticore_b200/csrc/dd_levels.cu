@@ -8,9 +8,17 @@
 // p*M + o keeps this linear: after the emit levels, problem k has drift
 // k + (M1*...*Mk)*db and final offsets 16k + r, so the last level is one launch of the
 // fused max kernel over all problems (dd_tree.cu, one staged window per problem).
-// Each emit level reads and writes Tr*N floats per drift block; the pairing of the adds
-// is the tree's own, so every path sum is bit-identical to the reference's
-// twoStageTaylorTree (taylor.cu:298-327).
+//
+// The default levels are emit_kernel's 4- and 2-row sums (one thread per channel,
+// coalesced).  A plan may instead start with the emitting form of the fused tree
+// (M = 16): each CTA stages a tile of 16 rows once for two drift blocks and writes all 16
+// in-block offsets of every channel, which moves the least data (one staged read of the
+// input per pair of drift blocks, one write and one read of the planes per drift block)
+// but stores each lane's strip with a 33-float stride, so its writes reach L2 as partial
+// sectors.  Measured on 64 x 256 x 131072 it ran at 41 Gsamples/s against 72 for the
+// default, so only the pool's autotuner, which times both per shape, may pick it.  The
+// pairing of the adds is the tree's own at every level, so every path sum is
+// bit-identical to the reference's twoStageTaylorTree (taylor.cu:298-327).
 #include "dd_common.cuh"
 #include "dd_internal.h"
 
@@ -25,7 +33,7 @@ __device__ __forceinline__ float ld_or_zero(const float* row, long long c, int N
 // One level of M in {2, 4} rows for every problem.  blockIdx.y = p*(Tp/M) + q.
 template <int M>
 __global__ void emit_kernel(const float* __restrict__ src, long long src_stride, int Tp, int D0,
-                            float* __restrict__ dst, int N) {
+                            float* __restrict__ dst, long long dst_stride, int N) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= N) return;
   const int nb = Tp / M;
@@ -56,7 +64,58 @@ __global__ void emit_kernel(const float* __restrict__ src, long long src_stride,
     out[3] = a1 + b1y2;
   }
 #pragma unroll
-  for (int o = 0; o < M; ++o) dst[(((long long)p * M + o) * nb + q) * N + c] = out[o];
+  for (int o = 0; o < M; ++o) dst[(((long long)p * M + o) * nb + q) * dst_stride + c] = out[o];
+}
+
+}  // namespace
+
+namespace {
+
+// The fused max level over the problems left after the emit levels: problem k of drift
+// block db has drift k + dscale*db and rows src + k*final_rows*N (row stride N).
+TreeGroup final_group(const float* src, long long Np, int N, int final_rows, int P, long long dscale, int db, int Tr,
+                      float* top) {
+  TreeGroup tp{};
+  tp.rows = src;
+  tp.row_stride = Np;
+  tp.job_row_stride = (long long)final_rows * Np;
+  tp.N = N;
+  tp.d_first = (int)(dscale * db);
+  tp.d_step = 1;
+  tp.n_jobs = P;
+  tp.db_first = db;
+  tp.db_step = 0;
+  tp.off_base = 0;
+  tp.off_step = final_rows;
+  tp.elig_T1 = Tr - 1;
+  tp.top = top;
+  return tp;
+}
+
+// The emitting 16-row tree for drift blocks db0 .. db0 + nj - 1 of the input's Tr rows:
+// group q reads rows 16q .. 16q + 15 (one trapezoid for the nj drift blocks) and writes
+// plane r*(Tr/16) + q of drift block j to out + j*job_stride.
+cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long long Np, int db0, int nj,
+                   float* out, long long job_stride, int num_sms, cudaStream_t stream) {
+  const int nb = Tr / 16;
+  TreeBatch eb;
+  eb.count = nb;
+  eb.n_items = 0;
+  for (int q = 0; q < nb; ++q) {
+    TreeGroup& g = eb.g[q];
+    g = TreeGroup{};
+    g.rows = input + (long long)16 * q * row_stride;
+    g.row_stride = row_stride;
+    g.job_row_stride = 0;
+    g.N = N;
+    g.d_first = db0;
+    g.d_step = 1;
+    g.n_jobs = nj;
+    g.emit_out = out + (long long)q * Np;
+    g.emit_job_stride = job_stride;
+    g.emit_plane_stride = (long long)nb * Np;
+  }
+  return tree_emit_batch(eb, num_sms, stream);
 }
 
 }  // namespace
@@ -70,19 +129,41 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
   if (plan.n > 0) {
     int prod = plan.final_rows;
     for (int l = 0; l < plan.n; ++l) {
-      if (plan.m[l] != 2 && plan.m[l] != 4) return cudaErrorInvalidValue;
-      sizes[nlev++] = plan.m[l];
-      prod *= plan.m[l];
+      const int M = plan.m[l];
+      if (M != 2 && M != 4 && !(M == 16 && l == 0)) return cudaErrorInvalidValue;
+      sizes[nlev++] = M;
+      prod *= M;
     }
     final_rows = plan.final_rows;
     if (prod != Tr || (final_rows != 2 && final_rows != 4 && final_rows != 8 && final_rows != 16))
       return cudaErrorInvalidValue;
   } else {
+    // Default: 4- and 2-row levels down to a final 16 rows.
     for (int tp = Tr; tp > 16;) {
       const int M = (tp / 4 >= 16) ? 4 : 2;
       sizes[nlev++] = M;
       tp /= M;
     }
+  }
+  // scratch_b lies in the same allocation as scratch_a (the emitting level addresses both
+  // from scratch_a): job stride in floats.
+  const long long job_stride = scratch_b - scratch_a;
+  const long long Np = level_row_length(N);  // plane row length
+  cudaError_t err;
+  if (nlev == 1 && sizes[0] == 16) {
+    // Two drift blocks per pass: one staged input read emits both, one launch finishes both.
+    for (int db = dmin; db <= dmax; db += 2) {
+      const int nj = (dmax - db + 1) < 2 ? 1 : 2;
+      if ((err = emit16(input, row_stride, Tr, N, Np, db, nj, scratch_a, job_stride, num_sms, stream)) != cudaSuccess)
+        return err;
+      TreeBatch tb;
+      tb.count = nj;
+      tb.n_items = 0;
+      for (int j = 0; j < nj; ++j)
+        tb.g[j] = final_group(scratch_a + j * job_stride, Np, N, final_rows, 16, 16, db + j, Tr, top);
+      if ((err = tree_max_batch(tb, final_rows, num_sms, stream)) != cudaSuccess) return err;
+    }
+    return cudaGetLastError();
   }
   for (int db = dmin; db <= dmax; ++db) {
     const float* src = input;
@@ -92,12 +173,16 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     long long dscale = 1;  // product of the level sizes so far
     for (int l = 0; l < nlev; ++l) {
       const int M = sizes[l];
-      dim3 grid((N + 255) / 256, (unsigned)(P * (Tp / M)));
-      const int D0 = (int)(dscale * db);
-      if (M == 4) emit_kernel<4><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, N);
-      else emit_kernel<2><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, N);
+      if (M == 16) {
+        if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, job_stride, num_sms, stream)) != cudaSuccess) return err;
+      } else {
+        dim3 grid((N + 255) / 256, (unsigned)(P * (Tp / M)));
+        const int D0 = (int)(dscale * db);
+        if (M == 4) emit_kernel<4><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+        else emit_kernel<2><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+      }
       src = dst;
-      stride = N;
+      stride = Np;
       dst = (dst == scratch_a) ? scratch_b : scratch_a;
       P *= M;
       Tp /= M;
@@ -106,23 +191,8 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     TreeBatch tb;
     tb.count = 1;
     tb.n_items = 0;
-    TreeGroup& tp = tb.g[0];
-    tp = TreeGroup{};
-    tp.rows = src;
-    tp.row_stride = N;
-    tp.job_row_stride = (long long)final_rows * N;
-    tp.N = N;
-    tp.d_first = (int)(dscale * db);
-    tp.d_step = 1;
-    tp.n_jobs = P;
-    tp.db_first = db;
-    tp.db_step = 0;
-    tp.off_base = 0;
-    tp.off_step = final_rows;
-    tp.elig_T1 = Tr - 1;
-    tp.top = top;
-    cudaError_t err = tree_max_batch(tb, final_rows, num_sms, stream);
-    if (err != cudaSuccess) return err;
+    tb.g[0] = final_group(src, Np, N, final_rows, P, dscale, db, Tr, top);
+    if ((err = tree_max_batch(tb, final_rows, num_sms, stream)) != cudaSuccess) return err;
   }
   return cudaGetLastError();
 }

@@ -128,6 +128,19 @@ int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
 
 std::vector<scb::LevelPlan> level_candidates(int Tr) {
   std::vector<scb::LevelPlan> out;
+  // the emitting 16-row tree first (two drift blocks per staged read), then 4s / 2s
+  if (Tr >= 32) {
+    scb::LevelPlan pl{};
+    pl.m[pl.n++] = 16;
+    int rem = Tr / 16;
+    while (rem > 16 && pl.n < 12) {
+      const int m = (rem / 4 >= 16) ? 4 : 2;
+      pl.m[pl.n++] = m;
+      rem /= m;
+    }
+    pl.final_rows = rem;
+    out.push_back(pl);
+  }
   // emit levels of 4s then 2s (or 2s then 4s) down to a final of 16 or 8 rows
   for (int fin : {16, 8}) {
     for (int order = 0; order < 2; ++order) {
@@ -200,15 +213,15 @@ int ensure_device(sc_dd_pool* p, size_t arena, size_t lvl, size_t host) {
   if (lvl > p->lvl_floats) {
     cudaDeviceSynchronize();
     cudaFree(p->lvl_a);
-    cudaFree(p->lvl_b);
     p->lvl_a = p->lvl_b = nullptr;
     p->lvl_floats = 0;
     for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
     p->graphs.clear();
     p->seen.clear();
-    if ((e = cudaMalloc(&p->lvl_a, lvl * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&p->lvl_b, lvl * sizeof(float))) != cudaSuccess)
+    // Both level buffers in one allocation: the emitting level addresses them as one array.
+    if ((e = cudaMalloc(&p->lvl_a, 2 * lvl * sizeof(float))) != cudaSuccess)
       return pfail(SC_DD_ENOMEM, std::string("pool level buffers: ") + cudaGetErrorString(e));
+    p->lvl_b = p->lvl_a + lvl;
     p->lvl_floats = lvl;
   }
   if (host > p->host_bytes) {
@@ -282,7 +295,6 @@ int sc_dd_pool_destroy(sc_dd_pool* p) {
   for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
   cudaFree(p->arena);
   cudaFree(p->lvl_a);
-  cudaFree(p->lvl_b);
   if (p->host) cudaFreeHost(p->host);
   for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1})
     if (ev) cudaEventDestroy(ev);
@@ -380,7 +392,7 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
       i = j;
     }
     for (const Planned& pl : plans)
-      if (pl.es.Tr > 16) lvl_need = std::max(lvl_need, (size_t)pl.es.Tr * pl.es.N);
+      if (pl.es.Tr > 16) lvl_need = std::max(lvl_need, scb::level_buffer_floats(pl.es.Tr, pl.es.N));
   }
   size_t host_need = 0;
   for (auto& sb : subs)

@@ -20,7 +20,9 @@ U channels, and the values a later iteration still needs are carried in register
 the back edge.  Looping (rather than unrolling the whole strip) keeps the code of one
 offset half small enough for the instruction cache.  Each channel's outputs are folded into
 a running maximum (starting at 0, so NaN and negative sums never count) that fold_max()
-merges into the CTA's per-channel maxima in shared memory.
+merges into the CTA's per-channel maxima in shared memory.  The emitting form
+(taylor_strip_emit) hands every root value to a sink instead: the first level of a tree of
+more than 16 rows, whose output planes the next level reads.
 """
 import os
 import sys
@@ -47,7 +49,7 @@ def lead(R, lo, hi):
     return max(max(P) for (L, b, o), P in pos.items() if L == 1)
 
 
-def gen_strip_loop(R, lo, hi, U, ITERS):
+def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
     """Looped form: a prologue fills every node's window for step 0, then ITERS iterations
     of a U-step body; values still needed after an iteration are carried into the next
     (the loop-carried registers), and each iteration folds its U per-channel maxima into the
@@ -116,6 +118,10 @@ def gen_strip_loop(R, lo, hi, U, ITERS):
         for (_, _, o) in roots:
             sh = (o + 1) // 2
             outs.append(f"{body_name(R // 2, 0, o // 2, s)} + {body_name(R // 2, 1, o // 2, s + sh)}")
+        if emit:
+            for i, e in enumerate(outs):
+                body.append((s, R, f"    sink.put({i}, base + {s}, {e});"))
+            continue
         body.append((s, R, f"    float m{s} = 0.0f;"))
         for i, e in enumerate(outs):
             body.append((s, R, f"    const float o{s}_{i} = {e};"))
@@ -140,6 +146,10 @@ def gen_strip_loop(R, lo, hi, U, ITERS):
     lines += carry
     lines.append("  }")
     body_text = "\n".join(lines)
+    if emit:
+        return (f"template <typename Row, typename Sink>\n"
+                f"__device__ __forceinline__ void taylor_strip_emit_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
+                f"    const Row (&row)[{R}], Sink& sink) {{\n{body_text}\n}}\n")
     return (f"template <typename Row>\n__device__ __forceinline__ void taylor_strip_loop_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
             f"    const Row (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
 
@@ -149,12 +159,21 @@ def gen_strip_loop(R, lo, hi, U, ITERS):
 LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3)]
 
 
+# (R, offset parts, U, iterations) of the emitting form: every root value goes to a sink
+# (the level kernels' output planes) instead of a running maximum.
+EMIT_CONFIGS = [(16, 2, 11, 3)]
+
+
 def main(out_path):
     parts = ["// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n"]
     for R, nparts, U, IT in LOOP_CONFIGS:
         step = R // nparts
         for k in range(nparts):
             parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT))
+    for R, nparts, U, IT in EMIT_CONFIGS:
+        step = R // nparts
+        for k in range(nparts):
+            parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, emit=True))
     # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS>(row, mrow) for any element accessor.
     parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row>\n"
                  "__device__ __forceinline__ void taylor_strip_loop(const Row (&row)[R], float* __restrict__ mrow) {")
@@ -164,6 +183,15 @@ def main(out_path):
             lo, hi = k * step, (k + 1) * step
             parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT}) "
                          f"taylor_strip_loop_{R}_{lo}_{hi}_{U}_{IT}(row, mrow);")
+    parts.append("}")
+    parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row, typename Sink>\n"
+                 "__device__ __forceinline__ void taylor_strip_emit(const Row (&row)[R], Sink& sink) {")
+    for R, nparts, U, IT in EMIT_CONFIGS:
+        step = R // nparts
+        for k in range(nparts):
+            lo, hi = k * step, (k + 1) * step
+            parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT}) "
+                         f"taylor_strip_emit_{R}_{lo}_{hi}_{U}_{IT}(row, sink);")
     parts.append("}")
     text = "\n".join(parts)
     if os.path.exists(out_path) and open(out_path).read() == text:
