@@ -42,8 +42,8 @@ def build(force=False, verbose_ptxas=False):
     finally:
         sys.path.pop(0)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [gen, os.path.join(CSRC, "dd_common.cuh"), os.path.join(CSRC, "dd_internal.h"),
-                   os.path.join(ROOT, "include", "seticore_b200.h")]
+    deps = srcs + [gen, os.path.join(CSRC, "generated", "taylor_direct_gen.cuh"), os.path.join(CSRC, "dd_common.cuh"),
+                   os.path.join(CSRC, "dd_internal.h"), os.path.join(ROOT, "include", "seticore_b200.h")]
     objdir = os.path.join(HERE, "_lib", "obj")
     os.makedirs(objdir, exist_ok=True)
     objs = []

@@ -176,8 +176,11 @@ cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t st
 cudaError_t path_values(const float* input, long long row_stride, int Tr, int N, const int* index,
                         const int* drift_steps, float* out, int n, cudaStream_t stream);
 
-// How a tree of more than 16 rows is split: emit levels of m[0..n) rows (2 or 4 each),
-// then a fused max level of final_rows (2, 4, 8 or 16) rows.  n == 0: the default split.
+// How a tree of more than 16 rows is split: levels of m[0..n) rows each -- 2 or 4
+// (emit_kernel), 8 or 16 (direct_kernel, one thread per channel) or, first only,
+// kStreamEmit16 (the emitting form of the fused tree) -- then a fused max level of
+// final_rows (2, 4, 8 or 16) rows.  n == 0: the default split.
+constexpr int kStreamEmit16 = 1016;
 struct LevelPlan {
   int n;
   int m[12];

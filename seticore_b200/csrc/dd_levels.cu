@@ -24,6 +24,9 @@
 
 namespace scb {
 
+#include "generated/taylor_direct_gen.cuh"
+
+
 namespace {
 
 __device__ __forceinline__ float ld_or_zero(const float* row, long long c, int N) {
@@ -62,6 +65,38 @@ __global__ void emit_kernel(const float* __restrict__ src, long long src_stride,
     out[1] = a0 + b0y1;
     out[2] = a1 + b1y1;
     out[3] = a1 + b1y2;
+  }
+#pragma unroll
+  for (int o = 0; o < M; ++o) dst[(((long long)p * M + o) * nb + q) * dst_stride + c] = out[o];
+}
+
+// One level of M in {8, 16} rows, one thread per channel: all M in-block offsets of the
+// M-row subtree at channel c from its 136 (M = 16) or 36 (M = 8) leaves, in the tree's
+// pairing (taylor_direct_M, generated).  Loads of neighbouring threads overlap, so most
+// come from L1; the level reads its input from HBM once and writes the planes once.
+template <int M>
+__global__ void __launch_bounds__(128) direct_kernel(const float* __restrict__ src, long long src_stride, int Tp,
+                                                     int D0, float* __restrict__ dst, long long dst_stride, int N) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const int nb = Tp / M;
+  const int p = blockIdx.y / nb;
+  const int q = blockIdx.y - p * nb;
+  const long long D = (long long)D0 + p;
+  const float* r0 = src + ((long long)p * Tp + (long long)q * M) * src_stride;
+  float out[M];
+  // Leaves lie in [c + min(0, (M-1)D), c + (M-1) + max(0, (M-1)D)]: inside the row for
+  // most channels, which then load without bounds checks.
+  const long long span = (long long)(M - 1) * D;
+  const bool inside = c + (span < 0 ? span : 0) >= 0 && c + (M - 1) + (span > 0 ? span : 0) < N;
+  if (inside) {
+    auto ld = [&](int t, int pos) { return __ldg(r0 + t * src_stride + c + D * t + pos); };
+    if constexpr (M == 16) taylor_direct_16(ld, out);
+    else taylor_direct_8(ld, out);
+  } else {
+    auto ld = [&](int t, int pos) { return ld_or_zero(r0 + t * src_stride, c + pos + D * t, N); };
+    if constexpr (M == 16) taylor_direct_16(ld, out);
+    else taylor_direct_8(ld, out);
   }
 #pragma unroll
   for (int o = 0; o < M; ++o) dst[(((long long)p * M + o) * nb + q) * dst_stride + c] = out[o];
@@ -130,27 +165,30 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     int prod = plan.final_rows;
     for (int l = 0; l < plan.n; ++l) {
       const int M = plan.m[l];
-      if (M != 2 && M != 4 && !(M == 16 && l == 0)) return cudaErrorInvalidValue;
+      if (M != 2 && M != 4 && M != 8 && M != 16 && !(M == kStreamEmit16 && l == 0)) return cudaErrorInvalidValue;
       sizes[nlev++] = M;
-      prod *= M;
+      prod *= (M == kStreamEmit16) ? 16 : M;
     }
     final_rows = plan.final_rows;
     if (prod != Tr || (final_rows != 2 && final_rows != 4 && final_rows != 8 && final_rows != 16))
       return cudaErrorInvalidValue;
   } else {
-    // Default: 4- and 2-row levels down to a final 16 rows.
-    for (int tp = Tr; tp > 16;) {
+    // Default: the one-thread-per-channel 16-row level, then 4s and 2s down to at most 16.
+    int tp = Tr / 16;
+    sizes[nlev++] = 16;
+    while (tp > 16) {
       const int M = (tp / 4 >= 16) ? 4 : 2;
       sizes[nlev++] = M;
       tp /= M;
     }
+    final_rows = tp;
   }
   // scratch_b lies in the same allocation as scratch_a (the emitting level addresses both
   // from scratch_a): job stride in floats.
   const long long job_stride = scratch_b - scratch_a;
   const long long Np = level_row_length(N);  // plane row length
   cudaError_t err;
-  if (nlev == 1 && sizes[0] == 16) {
+  if (nlev == 1 && sizes[0] == kStreamEmit16) {
     // Two drift blocks per pass: one staged input read emits both, one launch finishes both.
     for (int db = dmin; db <= dmax; db += 2) {
       const int nj = (dmax - db + 1) < 2 ? 1 : 2;
@@ -172,12 +210,17 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
     int P = 1, Tp = Tr;
     long long dscale = 1;  // product of the level sizes so far
     for (int l = 0; l < nlev; ++l) {
-      const int M = sizes[l];
-      if (M == 16) {
+      int M = sizes[l];
+      const int D0 = (int)(dscale * db);
+      if (M == kStreamEmit16) {
+        M = 16;
         if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, job_stride, num_sms, stream)) != cudaSuccess) return err;
+      } else if (M >= 8) {
+        dim3 grid((N + 127) / 128, (unsigned)(P * (Tp / M)));
+        if (M == 16) direct_kernel<16><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+        else direct_kernel<8><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
       } else {
         dim3 grid((N + 255) / 256, (unsigned)(P * (Tp / M)));
-        const int D0 = (int)(dscale * db);
         if (M == 4) emit_kernel<4><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
         else emit_kernel<2><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
       }

@@ -128,18 +128,28 @@ int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
 
 std::vector<scb::LevelPlan> level_candidates(int Tr) {
   std::vector<scb::LevelPlan> out;
-  // the emitting 16-row tree first (two drift blocks per staged read), then 4s / 2s
+  // a 16-row first level (one thread per channel, or the emitting fused tree with two
+  // drift blocks per staged read), then 4s / 2s down to at most 16 rows
   if (Tr >= 32) {
-    scb::LevelPlan pl{};
-    pl.m[pl.n++] = 16;
-    int rem = Tr / 16;
-    while (rem > 16 && pl.n < 12) {
-      const int m = (rem / 4 >= 16) ? 4 : 2;
-      pl.m[pl.n++] = m;
-      rem /= m;
+    for (int first : {16, scb::kStreamEmit16}) {
+      scb::LevelPlan pl{};
+      pl.m[pl.n++] = first;
+      int rem = Tr / 16;
+      while (rem > 16 && pl.n < 12) {
+        const int m = (rem / 4 >= 16) ? 4 : 2;
+        pl.m[pl.n++] = m;
+        rem /= m;
+      }
+      pl.final_rows = rem;
+      out.push_back(pl);
     }
-    pl.final_rows = rem;
-    out.push_back(pl);
+    // the one-thread-per-channel 8-row level first, finishing in 16 or fewer rows
+    if (Tr / 8 <= 16) {
+      scb::LevelPlan pl{};
+      pl.m[pl.n++] = 8;
+      pl.final_rows = Tr / 8;
+      out.push_back(pl);
+    }
   }
   // emit levels of 4s then 2s (or 2s then 4s) down to a final of 16 or 8 rows
   for (int fin : {16, 8}) {

@@ -154,14 +154,46 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
             f"    const Row (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
 
 
+def gen_direct(M):
+    """All M root values of an M-row Taylor subtree at one channel, as straight-line code:
+    every (node, position) value the roots need is computed once (bottom-up) from leaf
+    loads ld(t, pos) (row t of the block at relative channel pos; the caller applies the
+    shear).  One thread per channel, so loads and stores of a warp are coalesced."""
+    pos = consumption(M, 0, M)
+    order = sorted(pos.keys(), key=lambda k: k[0])
+    lines = []
+
+    def nm(L, b, o, j):
+        return f"n{L}_{b}_{o}_{j}"
+
+    for (L, b, o) in order:
+        for j in sorted(pos[(L, b, o)]):
+            if L == 1:
+                lines.append(f"  const float {nm(L, b, o, j)} = ld({b}, {j});")
+            elif L < M:
+                sh = (o + 1) // 2
+                lines.append(f"  const float {nm(L, b, o, j)} = {nm(L // 2, 2 * b, o // 2, j)} + "
+                             f"{nm(L // 2, 2 * b + 1, o // 2, j + sh)};")
+            else:
+                sh = (o + 1) // 2
+                lines.append(f"  out[{o}] = {nm(L // 2, 2 * b, o // 2, j)} + {nm(L // 2, 2 * b + 1, o // 2, j + sh)};")
+    body = "\n".join(lines)
+    return (f"template <typename Ld>\n__device__ __forceinline__ void taylor_direct_{M}(const Ld& ld, "
+            f"float (&out)[{M}]) {{\n{body}\n}}\n")
+
+
 # (R, offset parts, U steps per iteration, iterations) compiled into the library; a strip is
 # S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks).
-LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3)]
+LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3),
+                # short strips (S = 11) for launches whose jobs each stage their own rows
+                (2, 1, 11, 1), (4, 1, 11, 1), (8, 1, 11, 1), (16, 2, 11, 1)]
 
 
 # (R, offset parts, U, iterations) of the emitting form: every root value goes to a sink
 # (the level kernels' output planes) instead of a running maximum.
 EMIT_CONFIGS = [(16, 2, 11, 3)]
+# Subtree sizes of the one-thread-per-channel level kernel (dd_levels.cu).
+DIRECT_SIZES = [8, 16]
 
 
 def main(out_path):
@@ -174,6 +206,7 @@ def main(out_path):
         step = R // nparts
         for k in range(nparts):
             parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, emit=True))
+
     # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS>(row, mrow) for any element accessor.
     parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row>\n"
                  "__device__ __forceinline__ void taylor_strip_loop(const Row (&row)[R], float* __restrict__ mrow) {")
@@ -193,10 +226,17 @@ def main(out_path):
             parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT}) "
                          f"taylor_strip_emit_{R}_{lo}_{hi}_{U}_{IT}(row, sink);")
     parts.append("}")
-    text = "\n".join(parts)
-    if os.path.exists(out_path) and open(out_path).read() == text:
+    _write(out_path, "\n".join(parts))
+    direct = ["// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n"]
+    for M in DIRECT_SIZES:
+        direct.append(gen_direct(M))
+    _write(os.path.join(os.path.dirname(out_path), "taylor_direct_gen.cuh"), "\n".join(direct))
+
+
+def _write(path, text):
+    if os.path.exists(path) and open(path).read() == text:
         return
-    with open(out_path, "w") as f:
+    with open(path, "w") as f:
         f.write(text)
 
 
