@@ -7,6 +7,8 @@ import ctypes
 import os
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libseticore_b200.so")
+# SETICORE_B200_LIBRARY overrides the path (e.g. to compare builds of the library).
+LIB_PATH = os.environ.get("SETICORE_B200_LIBRARY", LIB_PATH)
 
 SC_DD_OK = 0
 SC_DD_EINVAL = 1

@@ -75,7 +75,7 @@ __global__ void emit_kernel(const float* __restrict__ src, long long src_stride,
 // pairing (taylor_direct_M, generated).  Loads of neighbouring threads overlap, so most
 // come from L1; the level reads its input from HBM once and writes the planes once.
 template <int M>
-__global__ void __launch_bounds__(128) direct_kernel(const float* __restrict__ src, long long src_stride, int Tp,
+__global__ void __launch_bounds__(128, 6) direct_kernel(const float* __restrict__ src, long long src_stride, int Tp,
                                                      int D0, float* __restrict__ dst, long long dst_stride, int N) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= N) return;

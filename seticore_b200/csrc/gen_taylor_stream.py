@@ -159,24 +159,32 @@ def gen_direct(M):
     every (node, position) value the roots need is computed once (bottom-up) from leaf
     loads ld(t, pos) (row t of the block at relative channel pos; the caller applies the
     shear).  One thread per channel, so loads and stores of a warp are coalesced."""
-    pos = consumption(M, 0, M)
-    order = sorted(pos.keys(), key=lambda k: k[0])
     lines = []
+    done = set()
 
     def nm(L, b, o, j):
         return f"n{L}_{b}_{o}_{j}"
 
-    for (L, b, o) in order:
-        for j in sorted(pos[(L, b, o)]):
-            if L == 1:
-                lines.append(f"  const float {nm(L, b, o, j)} = ld({b}, {j});")
-            elif L < M:
-                sh = (o + 1) // 2
-                lines.append(f"  const float {nm(L, b, o, j)} = {nm(L // 2, 2 * b, o // 2, j)} + "
-                             f"{nm(L // 2, 2 * b + 1, o // 2, j + sh)};")
-            else:
-                sh = (o + 1) // 2
-                lines.append(f"  out[{o}] = {nm(L // 2, 2 * b, o // 2, j)} + {nm(L // 2, 2 * b + 1, o // 2, j + sh)};")
+    def emit(L, b, o, j):
+        """Depth-first: a value is computed right before its first use, so leaves are
+        loaded late and few values are live at once."""
+        if (L, b, o, j) in done:
+            return
+        if L > 1:
+            sh = (o + 1) // 2
+            emit(L // 2, 2 * b, o // 2, j)
+            emit(L // 2, 2 * b + 1, o // 2, j + sh)
+            expr = f"{nm(L // 2, 2 * b, o // 2, j)} + {nm(L // 2, 2 * b + 1, o // 2, j + sh)}"
+        else:
+            expr = f"ld({b}, {j})"
+        done.add((L, b, o, j))
+        if L == M:
+            lines.append(f"  out[{o}] = {expr};")
+        else:
+            lines.append(f"  const float {nm(L, b, o, j)} = {expr};")
+
+    for o in range(M):
+        emit(M, 0, o, 0)
     body = "\n".join(lines)
     return (f"template <typename Ld>\n__device__ __forceinline__ void taylor_direct_{M}(const Ld& ld, "
             f"float (&out)[{M}]) {{\n{body}\n}}\n")
