@@ -157,7 +157,7 @@ def _hit_keys(res):
     return [[(h.index, h.drift_steps, h.power) for h in hs] for hs in res]
 
 
-def _uneven_requests(torch, n, precision_t16="fp32", seed=4000):
+def _uneven_requests(torch, n, precision="fp32", seed=4000):
     """The uneven mix on the device: T in {16..256}, N in {2^16..2^20}, max_drift U(1, 10)."""
     from seticore_b200 import SearchRequest
     from seticore_b200.synthetic import config_uneven, make_filterbank_torch
@@ -166,15 +166,14 @@ def _uneven_requests(torch, n, precision_t16="fp32", seed=4000):
     for i, sp in enumerate(specs):
         x = make_filterbank_torch(sp)
         reqs.append(SearchRequest(x, sp.num_timesteps, sp.foff_mhz, sp.tsamp, sp.max_drift, sp.min_drift,
-                                  sp.snr_threshold, beam=-1, coarse_channel=i,
-                                  precision=precision_t16 if sp.rounded_timesteps <= 16 else "fp32"))
+                                  sp.snr_threshold, beam=-1, coarse_channel=i, precision=precision))
     torch.cuda.synchronize()
     return specs, reqs
 
 
 def _with_precision(reqs, prec):
     import dataclasses
-    return [dataclasses.replace(r, precision=prec if r.input.shape[0] <= 16 else "fp32") for r in reqs]
+    return [dataclasses.replace(r, precision=prec) for r in reqs]
 
 
 def _time_pool(torch, pool, reqs, steps, warmup, stream):
@@ -192,8 +191,8 @@ def _time_pool(torch, pool, reqs, steps, warmup, stream):
 
 def run_uneven(args, world, rank, local):
     """Batched uneven searches through the pool (sc_dd_pool): autotuned on the first call,
-    captured as CUDA graphs on the second, replayed afterwards; FP32, and BF16 storage for
-    the searches of 16 timesteps (the 16-bit forms cover up to 16 rounded timesteps)."""
+    captured as CUDA graphs on the second, replayed afterwards; FP32 and BF16 storage (the
+    whole mix, and the searches of 16 timesteps on their own)."""
     import torch
     from seticore_b200 import SearchPool
     n = args.count or 512
@@ -238,7 +237,7 @@ def run_uneven(args, world, rank, local):
         sub["searches"] = len(t16)
         sub["samples_per_step"] = s16
     out["t16_subset"] = sub
-    # The whole mix with BF16 storage where it applies.
+    # The whole mix with BF16 storage.
     rq = _with_precision(reqs, "bf16")
     p = SearchPool(scratch_budget_bytes=16 << 30)
     m, r = _time_pool(torch, p, rq, args.steps, args.warmup, stream)
@@ -331,12 +330,32 @@ def run_beams(args, world, rank, local):
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
     samples = n * sp.rounded_timesteps * sp.num_channels
+    keys32 = _hit_keys(res)
+    precision = {}
+    for prec in ["bf16", "fp16"]:
+        dd.set_precision(prec)
+        for _ in range(max(3, args.warmup)):
+            got = dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold,
+                                      stream=stream)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold, stream=stream)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        st = dd.last_stats()
+        p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
+        precision[prec] = {"value": world * n * sp.rounded_timesteps * sp.num_channels / (p_ms / 1e3) / 1e9,
+                           "ms_per_step": p_ms, "hits_identical_to_fp32": _hit_keys(got) == keys32,
+                           "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}"}
+    dd.set_precision("fp32")
     out = {"metric": "dedoppler Gsamples/s (FP32, 64 beams x 256 x 131072)", "value": world * samples / (ms / 1e3) / 1e9,
            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"beams: {n} x 256 x 131072, foff 3.81 Hz, tsamp 0.268 s, max_drift 10 Hz/s",
                       "drift_blocks": sp.num_drift_blocks(), "input_bytes": samples * 4},
-           "clocks": clk, "hits_per_step": sum(len(h) for h in res)}
+           "clocks": clk, "hits_per_step": sum(len(h) for h in res), "precision_forms": precision}
     dd.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -440,7 +459,7 @@ def main():
         p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
         precision[prec] = {"value": world * samples_per_step / (p_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": p_ms,
                            "hits_identical_to_fp32": identical,
-                           "recomputed_tiles_first_search": f"{st.recomputed_tiles}/{st.total_tiles}",
+                           "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}",
                            "speedup_vs_fp32": ms / p_ms}
     dd.set_precision("fp32")
 

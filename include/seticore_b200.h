@@ -61,8 +61,8 @@ typedef struct sc_dd_stats {
   float tree_ms;      /* device time of the Taylor-tree kernel(s), CUDA events on the stream */
   float search_ms;    /* device time of the whole search, first memset to last kernel */
   int precision;          /* SC_DD_PRECISION_* of the search */
-  int recomputed_tiles;   /* precision form: tiles recomputed exactly in FP32 */
-  int total_tiles;        /* tiles of W channels in a coarse channel */
+  int recomputed_channels; /* precision form: channels whose top was recomputed in FP32 */
+  int total_channels;      /* channels of the search */
   int pad;
   double norm_mean;       /* precision form: FP64 mean of the power, used to normalise */
   double norm_std;        /* precision form: FP64 standard deviation, used to normalise */
@@ -123,8 +123,10 @@ int sc_dd_search_batch(sc_dd* dd, int count, const float* const* dev_inputs,
 int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_stride,
                                sc_dd_hit* hits, int num_hits, void* stream);
 
-/* Selects the storage form of later searches (SC_DD_PRECISION_*).  The 16-bit forms
- * support up to 16 rounded timesteps; they allocate their scratch on first use. */
+/* Selects the storage form of later searches (SC_DD_PRECISION_*).  The 16-bit forms store
+ * the FP64-normalised power as BF16 or FP16, sum it in FP32, and recompute in FP32, from
+ * the original power, the top of every channel within 0.9 x the threshold, so their hit
+ * lists equal the FP32 form's.  They allocate their scratch on first use. */
 int sc_dd_set_precision(sc_dd* dd, int precision);
 
 /* Statistics of the first search of the engine's last completed call; tree_ms and

@@ -93,8 +93,8 @@ class ScDdStats(ctypes.Structure):
         ("tree_ms", ctypes.c_float),
         ("search_ms", ctypes.c_float),
         ("precision", ctypes.c_int),
-        ("recomputed_tiles", ctypes.c_int),
-        ("total_tiles", ctypes.c_int),
+        ("recomputed_channels", ctypes.c_int),
+        ("total_channels", ctypes.c_int),
         ("pad", ctypes.c_int),
         ("norm_mean", ctypes.c_double),
         ("norm_std", ctypes.c_double),

@@ -113,13 +113,12 @@ struct sc_dd {
   int prec_slots = 0;
   void* norm16 = nullptr;        // [slot][Tr][N] 16-bit
   float* top16 = nullptr;        // [slot][N]
-  int* tiles = nullptr;          // [slot][max_tiles]
-  int* tile_counts = nullptr;    // [slot]
+  int* flags = nullptr;          // [slot][N] flagged channels
+  int* flag_counts = nullptr;    // [slot]
   double* norm_moments = nullptr;  // [slot][2 * kVarChunks + 2]
   unsigned* norm_tickets = nullptr;  // [slot]
-  int* host_tile_counts = nullptr;   // pinned [slot]
+  int* host_flag_counts = nullptr;   // pinned [slot]
   double* host_norm = nullptr;       // pinned [2]: mean, std of search 0
-  int max_tiles = 0;
   size_t device_bytes = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, tree start/end, call end
   sc_dd_stats last{};
@@ -167,13 +166,13 @@ void free_prec(sc_dd* d) {
   const size_t S = d->prec_slots, N = d->N;
   dfree(d, &d->norm16, 2 * N * d->Tr * S);
   dfree(d, &d->top16, sizeof(float) * N * S);
-  dfree(d, &d->tiles, sizeof(int) * d->max_tiles * S);
-  dfree(d, &d->tile_counts, sizeof(int) * S);
+  dfree(d, &d->flags, sizeof(int) * N * S);
+  dfree(d, &d->flag_counts, sizeof(int) * S);
   dfree(d, &d->norm_moments, sizeof(double) * (2 * scb::kVarChunks + 2) * S);
   dfree(d, &d->norm_tickets, sizeof(unsigned) * S);
-  if (d->host_tile_counts) cudaFreeHost(d->host_tile_counts);
+  if (d->host_flag_counts) cudaFreeHost(d->host_flag_counts);
   if (d->host_norm) cudaFreeHost(d->host_norm);
-  d->host_tile_counts = nullptr;
+  d->host_flag_counts = nullptr;
   d->host_norm = nullptr;
   d->prec_slots = 0;
 }
@@ -183,15 +182,14 @@ int ensure_prec(sc_dd* d, int slots) {
   cudaDeviceSynchronize();
   free_prec(d);
   const size_t S = slots, N = d->N;
-  d->max_tiles = (d->N + scb::tree_tile_width() - 1) / scb::tree_tile_width();
   cudaError_t e;
   if ((e = dalloc(d, &d->norm16, 2 * N * d->Tr * S)) != cudaSuccess ||
       (e = dalloc(d, &d->top16, sizeof(float) * N * S)) != cudaSuccess ||
-      (e = dalloc(d, &d->tiles, sizeof(int) * d->max_tiles * S)) != cudaSuccess ||
-      (e = dalloc(d, &d->tile_counts, sizeof(int) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->flags, sizeof(int) * N * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->flag_counts, sizeof(int) * S)) != cudaSuccess ||
       (e = dalloc(d, &d->norm_moments, sizeof(double) * (2 * scb::kVarChunks + 2) * S)) != cudaSuccess ||
       (e = dalloc(d, &d->norm_tickets, sizeof(unsigned) * S)) != cudaSuccess ||
-      (e = cudaMallocHost(&d->host_tile_counts, sizeof(int) * S)) != cudaSuccess ||
+      (e = cudaMallocHost(&d->host_flag_counts, sizeof(int) * S)) != cudaSuccess ||
       (e = cudaMallocHost(&d->host_norm, sizeof(double) * 2)) != cudaSuccess) {
     d->prec_slots = slots;
     free_prec(d);
@@ -297,8 +295,8 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
     if (prec) {
       q.norm16 = static_cast<char*>(dd->norm16) + (size_t)2 * dd->N * dd->Tr * k;
       q.top16 = dd->top16 + N * k;
-      q.tiles = dd->tiles + (size_t)dd->max_tiles * k;
-      q.tile_count = dd->tile_counts + k;
+      q.flags = dd->flags + N * k;
+      q.flag_count = dd->flag_counts + k;
       q.norm_moments = dd->norm_moments + (size_t)(2 * scb::kVarChunks + 2) * k;
       q.norm_ticket = dd->norm_tickets + k;
     }
@@ -332,10 +330,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
   int rc = ensure_slots(dd, std::min(count, scb::kMaxBatch), (int)std::min<long long>(nwin + 1, N / 2 + 2));
   if (rc != SC_DD_OK) return rc;
   const bool prec = dd->precision != SC_DD_PRECISION_FP32;
-  if (prec) {
-    if (Tr > 16) return fail(SC_DD_EINVAL, "the 16-bit forms support up to 16 rounded timesteps");
-    if ((rc = ensure_prec(dd, std::min(count, scb::kMaxBatch))) != SC_DD_OK) return rc;
-  }
+  if (prec && (rc = ensure_prec(dd, std::min(count, scb::kMaxBatch))) != SC_DD_OK) return rc;
   cudaError_t e;
   if ((e = cudaEventRecord(dd->ev[0], stream)) != cudaSuccess) return cuda_fail(e, "event");
   int total = 0;
@@ -351,7 +346,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
         (e = cudaMemcpy2DAsync(dd->host_cands(), sizeof(scb::Candidate) * kHostCands, dd->cands,
                                sizeof(scb::Candidate) * dd->cand_cap, sizeof(scb::Candidate) * head, n,
                                cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-        (prec && (e = cudaMemcpyAsync(dd->host_tile_counts, dd->tile_counts, sizeof(int) * n, cudaMemcpyDeviceToHost,
+        (prec && (e = cudaMemcpyAsync(dd->host_flag_counts, dd->flag_counts, sizeof(int) * n, cudaMemcpyDeviceToHost,
                                       stream)) != cudaSuccess) ||
         (prec && k0 == 0 &&
          (e = cudaMemcpyAsync(dd->host_norm, dd->norm_moments + 2 * scb::kVarChunks, sizeof(double) * 2,
@@ -383,8 +378,8 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
         dd->last.max_drift_block = p.dmax;
         dd->last.num_candidates = ncand;
         dd->last.precision = dd->precision;
-        dd->last.total_tiles = (N + scb::tree_tile_width() - 1) / scb::tree_tile_width();
-        dd->last.recomputed_tiles = prec ? dd->host_tile_counts[0] : dd->last.total_tiles;
+        dd->last.total_channels = N;
+        dd->last.recomputed_channels = prec ? dd->host_flag_counts[0] : N;
         dd->last.norm_mean = prec ? dd->host_norm[0] : 0.0;
         dd->last.norm_std = prec ? dd->host_norm[1] : 0.0;
       }
@@ -550,8 +545,6 @@ int sc_dd_set_precision(sc_dd* dd, int precision) {
   if (!dd) return fail(SC_DD_EINVAL, "sc_dd_set_precision: null engine");
   if (precision != SC_DD_PRECISION_FP32 && precision != SC_DD_PRECISION_BF16 && precision != SC_DD_PRECISION_FP16)
     return fail(SC_DD_EINVAL, "sc_dd_set_precision: unknown precision");
-  if (precision != SC_DD_PRECISION_FP32 && dd->Tr > 16)
-    return fail(SC_DD_EINVAL, "sc_dd_set_precision: the 16-bit forms support up to 16 rounded timesteps");
   dd->precision = precision;
   return SC_DD_OK;
 }

@@ -4,7 +4,8 @@
 // The searches travel in batches of up to kMaxBatch as kernel parameters, so a call is a
 // fixed sequence of launches (capturable in a CUDA graph) whatever the mix:
 //   clear -> [normalise] -> statistics -> tree launches grouped by (rows, element type)
-//   (levels for more than 16 rows, one search at a time) -> [flag + FP32 recompute] -> hits
+//   (levels for more than 16 rows, one search at a time) -> [flag + FP32 recompute of the
+//   flagged channels] -> hits
 #include <algorithm>
 
 #include "dd_common.cuh"
@@ -15,18 +16,18 @@ namespace scb {
 namespace {
 
 // Zeroes, per search of the batch: top (and the 16-bit tops), the result header and the
-// flagged-tile count.
+// flagged-channel count.
 __global__ void clear_kernel(const __grid_constant__ SearchBatch b, const __grid_constant__ PrecisionBatch pb) {
   const SearchDesc& d = b.s[blockIdx.y];
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) d.top[c] = 0.0f;
   if (blockIdx.x == 0 && threadIdx.x < (int)(sizeof(SearchHeader) / 4))
     reinterpret_cast<int*>(d.hdr)[threadIdx.x] = 0;
-  if (pb.count > 0 && blockIdx.y < (unsigned)pb.count && pb.s[blockIdx.y].tile_count) {
+  if (pb.count > 0 && blockIdx.y < (unsigned)pb.count && pb.s[blockIdx.y].flag_count) {
     const PrecisionDesc& q = pb.s[blockIdx.y];
     float* t16 = const_cast<float*>(q.top16);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < q.N; c += gridDim.x * blockDim.x) t16[c] = 0.0f;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      *q.tile_count = 0;
+      *q.flag_count = 0;
       *q.ticket = 0;
     }
   }
@@ -69,8 +70,11 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
   q.top16 = e.top16;
   q.hdr = hdr;
   q.snr_threshold = e.snr_threshold;
-  q.tile_list = e.tiles;
-  q.tile_count = e.tile_count;
+  q.dmin = e.dmin;
+  q.dmax = e.dmax;
+  q.top = e.top;
+  q.flag_list = e.flags;
+  q.flag_count = e.flag_count;
   return q;
 }
 
@@ -153,15 +157,23 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
           return e;
       }
     }
-    // More than 16 rows: the level path, one search at a time (shared level buffers).
+    // More than 16 rows: the level path, one search at a time (shared level buffers); the
+    // 16-bit searches run it on their normalised copy, with the default split.
     for (int k = 0; k < m; ++k) {
       if (ss[k].Tr <= 16) continue;
+      if (ss[k].elem != kElemF32) {
+        if ((e = levels_search(ss[k].norm16, ss[k].N, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
+                               ss[k].top16, num_sms, stream, LevelPlan{}, ss[k].elem)) != cudaSuccess)
+          return e;
+        continue;
+      }
       const LevelPlan plan = hooks.level_plan ? hooks.level_plan(hooks.ctx, ss[k], lvl_a, lvl_b, stream) : ss[k].level_plan;
       if ((e = levels_search(ss[k].input, ss[k].row_stride, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
                              ss[k].top, num_sms, stream, plan)) != cudaSuccess)
         return e;
     }
-    // The 16-bit searches: flag tiles near the threshold, recompute them exactly in FP32.
+    // The 16-bit searches: list the channels near the threshold, recompute them exactly
+    // in FP32 from the original power.
     {
       PrecisionBatch q;
       q.count = 0;
@@ -173,22 +185,8 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
           q.maxN = std::max(q.maxN, ss[k].N);
         }
       if (q.count) {
-        if ((e = flag_tiles_batch(q, tree_tile_width(), stream)) != cudaSuccess) return e;
-        for (int R : {2, 4, 8, 16}) {
-          TreeBatch tb;
-          tb.count = 0;
-          tb.n_items = 0;
-          for (int k = 0; k < m; ++k) {
-            if (ss[k].Tr != R || ss[k].elem == kElemF32) continue;
-            TreeGroup g = tree_group(ss[k], ss[k].input, ss[k].row_stride, ss[k].top);
-            g.tile_list = ss[k].tiles;
-            g.tile_count = ss[k].tile_count;
-            tb.g[tb.count++] = g;
-          }
-          if (tb.count && (e = tree_max_batch(tb, R, num_sms, stream, kElemF32,
-                                              hooks.budget_kb(hooks.ctx, tb, R, kElemF32))) != cudaSuccess)
-            return e;
-        }
+        if ((e = flag_channels_batch(q, num_sms, stream)) != cudaSuccess) return e;
+        if ((e = recompute_batch(q, num_sms, stream)) != cudaSuccess) return e;
       }
     }
     if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);
@@ -202,8 +200,7 @@ size_t ExecSearch::scratch_bytes(int Tr, int N, int cand_cap, int n_partials, in
   size_t b = a(sizeof(float) * N) * 2 + a(sizeof(SelectState)) + a(sizeof(MomentPartial) * n_partials) +
              a(sizeof(double) * 2 * kVarChunks) + a(sizeof(SearchHeader)) + a(sizeof(Candidate) * cand_cap);
   if (elem != kElemF32) {
-    const int tiles = (N + tree_tile_width() - 1) / tree_tile_width();
-    b += a((size_t)2 * Tr * N) + a(sizeof(float) * N) + a(sizeof(int) * tiles) + a(sizeof(int)) +
+    b += a((size_t)2 * Tr * N) + a(sizeof(float) * N) + a(sizeof(int) * N) + a(sizeof(int)) +
          a(sizeof(double) * (2 * kVarChunks + 2)) + a(sizeof(unsigned));
   }
   return b;
@@ -227,14 +224,13 @@ void ExecSearch::carve(char* base, int n_partials) {
   cands = reinterpret_cast<Candidate*>(p);
   p += a(sizeof(Candidate) * cand_cap);
   if (elem != kElemF32) {
-    const int tiles_n = (N + tree_tile_width() - 1) / tree_tile_width();
     norm16 = p;
     p += a((size_t)2 * Tr * N);
     top16 = reinterpret_cast<float*>(p);
     p += a(sizeof(float) * N);
-    tiles = reinterpret_cast<int*>(p);
-    p += a(sizeof(int) * tiles_n);
-    tile_count = reinterpret_cast<int*>(p);
+    flags = reinterpret_cast<int*>(p);
+    p += a(sizeof(int) * N);
+    flag_count = reinterpret_cast<int*>(p);
     p += a(sizeof(int));
     norm_moments = reinterpret_cast<double*>(p);
     p += a(sizeof(double) * (2 * kVarChunks + 2));

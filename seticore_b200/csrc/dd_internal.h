@@ -152,8 +152,10 @@ struct PrecisionDesc {
   const float* top16;   // tops of the 16-bit tree (normalised units)
   const SearchHeader* hdr;
   double snr_threshold;
-  int* tile_list;       // flagged tiles
-  int* tile_count;
+  int dmin, dmax;       // drift blocks
+  float* top;           // exact float32 tops of the flagged channels (others stay 0)
+  int* flag_list;       // flagged channels (capacity N)
+  int* flag_count;
 };
 struct PrecisionBatch {
   int count;
@@ -163,8 +165,11 @@ struct PrecisionBatch {
 };
 // FP64 mean and standard deviation of the unrounded rows, then the normalised copy.
 cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
-// Flags every tile holding a channel whose 16-bit top reaches 0.9 x the threshold.
-cudaError_t flag_tiles_batch(const PrecisionBatch& b, int tile_width, cudaStream_t stream);
+// Lists every channel whose 16-bit top reaches 0.9 x the threshold.
+cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
+// The exact float32 top of every listed channel: each eligible path summed from the
+// original power in the tree's pairing, the maximum floored at 0.
+cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
 
 // Column sums, order statistics, mean, standard deviation and threshold of each search.
 cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
@@ -190,9 +195,11 @@ struct LevelPlan {
 // Multi-level tree for Tr > 16 (one search): level kernels write the partial planes of
 // every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).
 // scratch_a / scratch_b: level_buffer_floats(Tr, N) floats each, in one allocation.
-cudaError_t levels_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
+// `input` holds elements of type `elem` (float, or the precision form's 16-bit copy, which
+// only the default plan reads: its first level converts on load).
+cudaError_t levels_search(const void* input, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
-                          cudaStream_t stream, const LevelPlan& plan = LevelPlan{});
+                          cudaStream_t stream, const LevelPlan& plan = LevelPlan{}, int elem = kElemF32);
 
 // A fully planned search for exec_queue: the request, its drift plan and its scratch.
 struct ExecSearch {
@@ -214,8 +221,8 @@ struct ExecSearch {
   Candidate* cands;
   void* norm16;
   float* top16;
-  int* tiles;
-  int* tile_count;
+  int* flags;       // flagged channels (N)
+  int* flag_count;
   double* norm_moments;
   unsigned* norm_ticket;
   static size_t scratch_bytes(int Tr, int N, int cand_cap, int n_partials, int elem);

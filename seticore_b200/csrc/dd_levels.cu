@@ -19,6 +19,9 @@
 // default, so only the pool's autotuner, which times both per shape, may pick it.  The
 // pairing of the adds is the tree's own at every level, so every path sum is
 // bit-identical to the reference's twoStageTaylorTree (taylor.cu:298-327).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "dd_common.cuh"
 #include "dd_internal.h"
 
@@ -29,8 +32,13 @@ namespace scb {
 
 namespace {
 
-__device__ __forceinline__ float ld_or_zero(const float* row, long long c, int N) {
-  return (c >= 0 && c < N) ? __ldg(row + c) : 0.0f;
+__device__ __forceinline__ float as_float(float v) { return v; }
+__device__ __forceinline__ float as_float(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float as_float(__half v) { return __half2float(v); }
+
+template <typename E>
+__device__ __forceinline__ float ld_or_zero(const E* row, long long c, int N) {
+  return (c >= 0 && c < N) ? as_float(row[c]) : 0.0f;
 }
 
 // One level of M in {2, 4} rows for every problem.  blockIdx.y = p*(Tp/M) + q.
@@ -74,23 +82,23 @@ __global__ void emit_kernel(const float* __restrict__ src, long long src_stride,
 // M-row subtree at channel c from its 136 (M = 16) or 36 (M = 8) leaves, in the tree's
 // pairing (taylor_direct_M, generated).  Loads of neighbouring threads overlap, so most
 // come from L1; the level reads its input from HBM once and writes the planes once.
-template <int M>
-__global__ void __launch_bounds__(128, 6) direct_kernel(const float* __restrict__ src, long long src_stride, int Tp,
-                                                     int D0, float* __restrict__ dst, long long dst_stride, int N) {
+template <int M, typename E>
+__global__ void __launch_bounds__(128, 6) direct_kernel(const E* __restrict__ src, long long src_stride, int Tp,
+                                                        int D0, float* __restrict__ dst, long long dst_stride, int N) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= N) return;
   const int nb = Tp / M;
   const int p = blockIdx.y / nb;
   const int q = blockIdx.y - p * nb;
   const long long D = (long long)D0 + p;
-  const float* r0 = src + ((long long)p * Tp + (long long)q * M) * src_stride;
+  const E* r0 = src + ((long long)p * Tp + (long long)q * M) * src_stride;
   float out[M];
   // Leaves lie in [c + min(0, (M-1)D), c + (M-1) + max(0, (M-1)D)]: inside the row for
   // most channels, which then load without bounds checks.
   const long long span = (long long)(M - 1) * D;
   const bool inside = c + (span < 0 ? span : 0) >= 0 && c + (M - 1) + (span > 0 ? span : 0) < N;
   if (inside) {
-    auto ld = [&](int t, int pos) { return __ldg(r0 + t * src_stride + c + D * t + pos); };
+    auto ld = [&](int t, int pos) { return as_float(r0[t * src_stride + c + D * t + pos]); };
     if constexpr (M == 16) taylor_direct_16(ld, out);
     else taylor_direct_8(ld, out);
   } else {
@@ -155,12 +163,14 @@ cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long
 
 }  // namespace
 
-cudaError_t levels_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
+cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
-                          cudaStream_t stream, const LevelPlan& plan) {
+                          cudaStream_t stream, const LevelPlan& plan, int elem) {
   int sizes[12];
   int nlev = 0;
   int final_rows = 16;
+  const float* input = static_cast<const float*>(input_v);
+  if (elem != kElemF32 && plan.n > 0) return cudaErrorInvalidValue;  // 16-bit input: default split only
   if (plan.n > 0) {
     int prod = plan.final_rows;
     for (int l = 0; l < plan.n; ++l) {
@@ -217,8 +227,16 @@ cudaError_t levels_search(const float* input, long long row_stride, int Tr, int 
         if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, job_stride, num_sms, stream)) != cudaSuccess) return err;
       } else if (M >= 8) {
         dim3 grid((N + 127) / 128, (unsigned)(P * (Tp / M)));
-        if (M == 16) direct_kernel<16><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
-        else direct_kernel<8><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+        if (l == 0 && elem == kElemBF16) {
+          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __nv_bfloat16*>(input_v), stride, Tp, D0, dst,
+                                                     Np, N);
+        } else if (l == 0 && elem == kElemF16) {
+          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __half*>(input_v), stride, Tp, D0, dst, Np, N);
+        } else if (M == 16) {
+          direct_kernel<16><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+        } else {
+          direct_kernel<8><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+        }
       } else {
         dim3 grid((N + 255) / 256, (unsigned)(P * (Tp / M)));
         if (M == 4) emit_kernel<4><<<grid, 256, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);

@@ -376,8 +376,6 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
     q.snr_threshold = r.snr_threshold;
     q.elem = r.precision == SC_DD_PRECISION_BF16 ? scb::kElemBF16
              : r.precision == SC_DD_PRECISION_FP16 ? scb::kElemF16 : scb::kElemF32;
-    if (q.elem != scb::kElemF32 && q.Tr > 16)
-      return pfail(SC_DD_EINVAL, "sc_dd_pool_search: the 16-bit forms support up to 16 rounded timesteps");
     const long long nwin = ((long long)q.N + q.window_size - 1) / q.window_size;
     q.cand_cap = (int)std::min<long long>(nwin + 1, q.N / 2 + 2);
     pl.min_drift = r.min_drift;

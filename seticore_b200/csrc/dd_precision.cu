@@ -2,23 +2,26 @@
 //
 //   1. norm_moments_kernel: per search, the FP64 mean and standard deviation of the
 //      unrounded rows of the original float32 power (zero-padded rows excluded).
-//   2. normalize_kernel: y = (x - mean) / std, rounded to BF16 or FP16 (padded rows stay
-//      0), into a dense [Tr][N] 16-bit copy -- half the bytes of the float32 input.
-//   3. (dd_tree.cu) the fused tree over y, accumulating in FP32, gives approximate tops.
-//      A path sum of y equals (P - T*mean) / std for the path sum P of x, so the order of
-//      path sums is preserved up to the 16-bit rounding.
-//   4. flag_tiles_kernel: a tile is flagged if any of its channels has an approximate
-//      top at or above 0.9 x the threshold in SNR units: P >= median + 0.9 * snr * std.
-//   5. (dd_tree.cu) the FP32 tree runs again over the flagged tiles only, from the
-//      original power, writing exact tops (bit-identical to the plain form) there.
-//      Every other channel keeps top 0: its approximate top is below 0.9 x threshold, so
-//      its exact top is below the threshold and it can neither become a window
-//      candidate nor beat one (dedoppler.cu:353-383 compares only with values above
-//      the threshold).  The hit list is therefore the plain form's.
+//   2. normalize_kernel: y = (x - mean) / std in FP64, rounded to BF16 or FP16 (padded
+//      rows stay 0), into a dense [Tr][N] 16-bit copy -- half the bytes of the input.
+//   3. (dd_tree.cu, dd_levels.cu) the tree over y, accumulating in FP32, gives approximate
+//      tops.  A path sum of y equals (P - T*mean) / std for the path sum P of x, so the
+//      order of path sums is kept up to the 16-bit rounding.
+//   4. flag_channels_kernel: lists every channel whose approximate top reaches 0.9 x the
+//      threshold in SNR units, P >= median + 0.9 * snr * std, mapped to y units.
+//   5. recompute_kernel: for each listed channel, every eligible path is summed from the
+//      original power in the tree's own pairing (bit-identical to the plain form's tree)
+//      and the maximum, floored at 0, becomes its top.  Every other channel keeps top 0:
+//      its approximate top is below 0.9 x threshold, so its exact top is below the
+//      threshold and it can neither become a window candidate nor beat one
+//      (dedoppler.cu:353-383 compares only with values above the threshold).  The hit list
+//      is therefore the plain form's.
 // The statistics (median, standard deviation, threshold) always come from the float32
 // column sums, exactly as in the plain form.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <cstring>
 
 #include "dd_common.cuh"
 #include "dd_internal.h"
@@ -33,12 +36,27 @@ __global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
   __shared__ bool last_block;
   const long long total = (long long)d.T * d.N;
   double s1 = 0.0, s2 = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long t = i / d.N, c = i - t * d.N;
-    const double v = (double)__ldg(d.input + t * d.row_stride + c);
-    s1 += v;
-    s2 += v * v;
+  // Row by row, each thread over channels (128-bit loads when the rows allow them).
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  const bool vec = (d.N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
+  for (int t = 0; t < d.T; ++t) {
+    const float* row = d.input + (long long)t * d.row_stride;
+    if (vec) {
+      const float4* r4 = reinterpret_cast<const float4*>(row);
+      for (long long c = tid; c < d.N / 4; c += nth) {
+        const float4 v = __ldg(r4 + c);
+        const double a = v.x, b2 = v.y, c2 = v.z, e = v.w;
+        s1 += (a + b2) + (c2 + e);
+        s2 += (a * a + b2 * b2) + (c2 * c2 + e * e);
+      }
+    } else {
+      for (long long c = tid; c < d.N; c += nth) {
+        const double v = (double)__ldg(row + c);
+        s1 += v;
+        s2 += v * v;
+      }
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     s1 += __shfl_down_sync(0xffffffffu, s1, o);
@@ -111,35 +129,82 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
   const double mean = d.moments[2 * kVarChunks];
   const double inv = 1.0 / d.moments[2 * kVarChunks + 1];
   E* out = static_cast<E*>(d.norm);
-  const long long total = (long long)d.Tr * d.N;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long t = i / d.N, c = i - t * d.N;
-    float y = 0.0f;
-    if (t < d.T) y = (float)(((double)__ldg(d.input + t * d.row_stride + c) - mean) * inv);
-    out[i] = from_float<E>(y);
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  const bool vec = (d.N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
+  for (int t = 0; t < d.Tr; ++t) {
+    const float* row = d.input + (long long)t * d.row_stride;
+    E* orow = out + (long long)t * d.N;
+    if (vec) {
+      const float4* r4 = reinterpret_cast<const float4*>(row);
+      for (long long c = tid; c < d.N / 4; c += nth) {
+        E y[4] = {from_float<E>(0.0f), from_float<E>(0.0f), from_float<E>(0.0f), from_float<E>(0.0f)};
+        if (t < d.T) {
+          const float4 v = __ldg(r4 + c);
+          y[0] = from_float<E>((float)(((double)v.x - mean) * inv));
+          y[1] = from_float<E>((float)(((double)v.y - mean) * inv));
+          y[2] = from_float<E>((float)(((double)v.z - mean) * inv));
+          y[3] = from_float<E>((float)(((double)v.w - mean) * inv));
+        }
+        uint2 packed;
+        memcpy(&packed, y, sizeof(packed));
+        reinterpret_cast<uint2*>(orow)[c] = packed;
+      }
+    } else {
+      for (long long c = tid; c < d.N; c += nth) {
+        float y = 0.0f;
+        if (t < d.T) y = (float)(((double)__ldg(row + c) - mean) * inv);
+        orow[c] = from_float<E>(y);
+      }
+    }
   }
 }
 
-__global__ void flag_tiles_kernel(const __grid_constant__ PrecisionBatch b, int tile_width) {
+__global__ void flag_channels_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
-  __shared__ int any;
-  const int n_tiles = (d.N + tile_width - 1) / tile_width;
   // Loose threshold in SNR units (0.9 x), mapped to normalised path-sum units.
   const double median = (double)d.hdr->median, sd = (double)d.hdr->std_dev;
   const double mean = d.moments[2 * kVarChunks], scale = d.moments[2 * kVarChunks + 1];
   const double thr_x = median + 0.9 * d.snr_threshold * sd;
   const float thr_y = (float)((thr_x - (double)d.T * mean) / scale);
-  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    if (threadIdx.x == 0) any = 0;
-    __syncthreads();
-    const int c0 = tile * tile_width, c1 = min(d.N, c0 + tile_width);
-    bool hit = false;
-    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) hit |= !(d.top16[c] < thr_y);
-    if (__any_sync(0xffffffffu, hit) && (threadIdx.x & 31) == 0) any = 1;
-    __syncthreads();
-    if (threadIdx.x == 0 && any) d.tile_list[atomicAdd(d.tile_count, 1)] = tile;
-    __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int c0 = blockIdx.x * blockDim.x; c0 < d.N; c0 += gridDim.x * blockDim.x) {
+    const int c = c0 + threadIdx.x;
+    const bool f = c < d.N && !(d.top16[c] < thr_y);  // NaN is flagged
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    if (m) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(d.flag_count, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (f) d.flag_list[base + __popc(m & ((1u << lane) - 1u))] = c;
+    }
+  }
+}
+
+// One warp per listed channel, lanes over its (drift block, offset) paths.
+__global__ void recompute_kernel(const __grid_constant__ PrecisionBatch b) {
+  const PrecisionDesc& d = b.s[blockIdx.y];
+  const int n = *d.flag_count;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const int Tr = d.Tr, N = d.N;
+  const int paths = (d.dmax - d.dmin + 1) * Tr;
+  for (int k = blockIdx.x * wpb + (threadIdx.x >> 5); k < n; k += gridDim.x * wpb) {
+    const int c = d.flag_list[k];
+    float best = 0.0f;
+    for (int pth = lane; pth < paths; pth += 32) {
+      const int db = d.dmin + pth / Tr;
+      const int off = pth - (pth / Tr) * Tr;
+      const long long e = (long long)(Tr - 1) * db;
+      if (c + e < 0 || c + e + off >= N) continue;  // findTopPathSums' early return (dedoppler.cu:40-46)
+      const float* base = d.input + c;
+      const float v = path_sum_pairwise(Tr, off, [&](int t, int pos) {
+        return __ldg(base + (long long)t * d.row_stride + (long long)db * t + pos);
+      });
+      best = fmaxf(best, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) d.top[c] = best;
   }
 }
 
@@ -158,11 +223,20 @@ cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
   return cudaGetLastError();
 }
 
-cudaError_t flag_tiles_batch(const PrecisionBatch& b, int tile_width, cudaStream_t stream) {
+cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream) {
   if (b.count <= 0) return cudaSuccess;
-  const int n_tiles = (b.maxN + tile_width - 1) / tile_width;
-  int blocks = n_tiles < 1024 ? n_tiles : 1024;
-  flag_tiles_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b, tile_width);
+  int blocks = (b.maxN + 255) / 256;
+  const int cap = (4 * num_sms + b.count - 1) / b.count;
+  if (blocks > cap) blocks = cap < 1 ? 1 : cap;
+  flag_channels_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream) {
+  if (b.count <= 0) return cudaSuccess;
+  int blocks = (8 * num_sms + b.count - 1) / b.count;
+  if (blocks < 1) blocks = 1;
+  recompute_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
   return cudaGetLastError();
 }
 

@@ -30,7 +30,7 @@ def _mixed_requests(torch, n=24, seed=60):
         T = int(rng.choice([4, 8, 13, 16, 32, 64]))
         N = int(rng.choice([4096, 10000, 32768, 65536]))
         md = float(rng.uniform(0.5, 6.0))
-        prec = str(rng.choice(["fp32", "fp32", "bf16", "fp16"])) if T <= 16 else "fp32"
+        prec = str(rng.choice(["fp32", "fp32", "bf16", "fp16"]))
         spec = SearchSpec(T, N, tsamp=18.253611 * 16 / max(T, 16), max_drift=md, seed=seed * 100 + i,
                           n_tones=int(rng.integers(1, 6)), tone_drift=min(md, 4.0), snr_threshold=8.0)
         x = make_filterbank_torch(spec)

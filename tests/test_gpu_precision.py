@@ -26,7 +26,8 @@ def _hits(dd, xt, spec):
 
 
 CASES = [(16, 65536, 4.0, 1, 1), (16, 40000, 4.0, 2, 0), (8, 30000, 2.0, 3, 2), (13, 20000, 3.0, 4, 1),
-         (4, 50000, 1.0, 5, 1), (2, 20000, 1.0, 6, 0), (16, 1 << 20, 4.0, 7, 2)]
+         (4, 50000, 1.0, 5, 1), (2, 20000, 1.0, 6, 0), (16, 1 << 20, 4.0, 7, 2),
+         (32, 65536, 4.0, 8, 1), (100, 32768, 2.0, 9, 0), (256, 131072, 2.0, 10, 1)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"T{c[0]}_N{c[1]}_s{c[3]}")
@@ -45,7 +46,7 @@ def test_16bit_forms_return_the_fp32_hit_list(torch_cuda, case, precision):
     st = dd.last_stats()
     assert got == want
     assert len(want) >= 1
-    assert 0 < st.recomputed_tiles <= st.total_tiles
+    assert 0 < st.recomputed_channels <= st.total_channels
     # a second call on the same engine (scratch reuse) gives the same answer
     assert _hits(dd, xt, spec) == want
     dd.close()

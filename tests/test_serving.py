@@ -29,7 +29,7 @@ def test_served_results_equal_results_alone():
         spec = SearchSpec(T, N, tsamp=18.253611 * 16 / max(T, 16), max_drift=float(rng.uniform(1, 5)),
                           seed=7000 + i, n_tones=3, snr_threshold=8.0)
         reqs.append(SearchRequest(make_filterbank_torch(spec), T, spec.foff_mhz, spec.tsamp, spec.max_drift, 0.0,
-                                  8.0, coarse_channel=i, precision="bf16" if (T <= 16 and i % 3 == 0) else "fp32"))
+                                  8.0, coarse_channel=i, precision="bf16" if i % 3 == 0 else "fp32"))
     alone = []
     for r in reqs:
         dd = Dedopplerer(r.num_timesteps, r.input.shape[1], r.foff, r.tsamp)
