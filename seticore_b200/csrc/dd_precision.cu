@@ -9,9 +9,9 @@
 //      order of path sums is kept up to the 16-bit rounding.
 //   4. flag_channels_kernel: lists every channel whose approximate top reaches 0.9 x the
 //      threshold in SNR units, P >= median + 0.9 * snr * std, mapped to y units.
-//   5. recompute_kernel: for each listed channel, every eligible path is summed from the
-//      original power in the tree's own pairing (bit-identical to the plain form's tree)
-//      and the maximum, floored at 0, becomes its top.  Every other channel keeps top 0:
+//   5. recompute_kernel: for each listed channel, every eligible path is summed (one path
+//      per thread) from the original power in the tree's own pairing (bit-identical to the
+//      plain form's tree) and the maximum, floored at 0, becomes its top.  Every other channel keeps top 0:
 //      its approximate top is below 0.9 x threshold, so its exact top is below the
 //      threshold and it can neither become a window candidate nor beat one
 //      (dedoppler.cu:353-383 compares only with values above the threshold).  The hit list
@@ -181,30 +181,33 @@ __global__ void flag_channels_kernel(const __grid_constant__ PrecisionBatch b) {
   }
 }
 
-// One warp per listed channel, lanes over its (drift block, offset) paths.
+// Work unit = (listed channel, block of blockDim.x of its (drift block, offset) paths),
+// one path per thread; the channel's maximum meets in global memory (atomicMax on the
+// float bits: every candidate is >= 0).
 __global__ void recompute_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
-  const int n = *d.flag_count;
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
+  const long long n = *d.flag_count;
   const int Tr = d.Tr, N = d.N;
   const int paths = (d.dmax - d.dmin + 1) * Tr;
-  for (int k = blockIdx.x * wpb + (threadIdx.x >> 5); k < n; k += gridDim.x * wpb) {
+  const int nblk = (paths + blockDim.x - 1) / blockDim.x;
+  for (long long u = blockIdx.x; u < n * nblk; u += gridDim.x) {
+    const long long k = u / nblk;
+    const int pth = (int)(u - k * nblk) * blockDim.x + threadIdx.x;
     const int c = d.flag_list[k];
     float best = 0.0f;
-    for (int pth = lane; pth < paths; pth += 32) {
+    if (pth < paths) {
       const int db = d.dmin + pth / Tr;
       const int off = pth - (pth / Tr) * Tr;
       const long long e = (long long)(Tr - 1) * db;
-      if (c + e < 0 || c + e + off >= N) continue;  // findTopPathSums' early return (dedoppler.cu:40-46)
-      const float* base = d.input + c;
-      const float v = path_sum_pairwise(Tr, off, [&](int t, int pos) {
-        return __ldg(base + (long long)t * d.row_stride + (long long)db * t + pos);
-      });
-      best = fmaxf(best, v);
+      if (c + e >= 0 && c + e + off < N) {  // findTopPathSums' early return (dedoppler.cu:40-46)
+        const float* base = d.input + c;
+        best = fmaxf(0.0f, path_sum_pairwise(Tr, off, [&](int t, int pos) {
+          return __ldg(base + (long long)t * d.row_stride + (long long)db * t + pos);
+        }));
+      }
     }
     for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if (lane == 0) d.top[c] = best;
+    if ((threadIdx.x & 31) == 0 && best > 0.0f) atomicMax(reinterpret_cast<int*>(d.top) + c, __float_as_int(best));
   }
 }
 
@@ -234,7 +237,7 @@ cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream
 
 cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream) {
   if (b.count <= 0) return cudaSuccess;
-  int blocks = (8 * num_sms + b.count - 1) / b.count;
+  int blocks = (16 * num_sms + b.count - 1) / b.count;
   if (blocks < 1) blocks = 1;
   recompute_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
   return cudaGetLastError();

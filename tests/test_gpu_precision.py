@@ -69,26 +69,44 @@ def _fp64_top(oracle, x, spec):
     return top
 
 
-def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle):
-    """States the top-path-sum error of each form against the FP64 tree (printed), and
-    bounds it: FP32 1e-6, FP16 1e-3, BF16 1e-2 relative (to the top sum)."""
+ERROR_CASES = {
+    # the node's coarse-channel model (16 timesteps, GBT resolution), narrower for the oracle
+    "node_16": dict(T=16, N=32768, foff_hz=2.7939677, tsamp=18.253611, max_drift=4.0),
+    # the beamformed model (256 timesteps, 3.81 Hz, 0.268 s, 10 Hz/s)
+    "beams_256": dict(T=256, N=8192, foff_hz=1e6 / 262144, tsamp=0.268435456, max_drift=10.0),
+    # one of the uneven mix's shapes (64 timesteps, tsamp scaled to the same span)
+    "uneven_64": dict(T=64, N=16384, foff_hz=2.7939677, tsamp=18.253611 * 16 / 64, max_drift=6.0),
+}
+
+
+@pytest.mark.parametrize("name", list(ERROR_CASES))
+def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle, name):
+    """States the top-path-sum error of each form against the FP64 tree (printed as one JSON
+    line per case), and bounds it: FP32 1e-6, FP16 1e-3, BF16 1e-2 relative (to the top
+    sum), over the channels whose top is above the median top."""
+    import json
     from seticore_b200 import Dedopplerer
     from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
-    spec = SearchSpec(16, 32768, seed=77, n_tones=8, snr_threshold=8.0)
+    c = ERROR_CASES[name]
+    spec = SearchSpec(c["T"], c["N"], foff_hz=c["foff_hz"], tsamp=c["tsamp"], max_drift=c["max_drift"], seed=77,
+                      n_tones=8, tone_drift=min(c["max_drift"], 4.0), snr_threshold=8.0)
     x = make_filterbank_numpy(spec)
     ref = _fp64_top(port_oracle, x, spec)
     xt = torch_cuda.from_numpy(x).cuda()
-    dd = Dedopplerer(16, spec.num_channels, spec.foff_mhz, spec.tsamp)
+    dd = Dedopplerer(spec.num_timesteps, spec.num_channels, spec.foff_mhz, spec.tsamp)
     dd.search_raw(xt, -1, 0, spec.max_drift, 0.0, spec.snr_threshold)
     top32 = dd.channel_array("top").cpu().numpy().astype(np.float64)
-    err = {"fp32": np.max(np.abs(top32 - ref) / ref)}
+    sel = ref > np.percentile(ref, 50)  # the approximate tops are floored at 0 in normalised units
+    err = {"fp32": float(np.max(np.abs(top32[sel] - ref[sel]) / ref[sel]))}
     for prec, bound in (("fp16", 1e-3), ("bf16", 1e-2)):
         dd.set_precision(prec)
         dd.search_raw(xt, -1, 0, spec.max_drift, 0.0, spec.snr_threshold)
         st = dd.last_stats()
-        approx = dd.channel_array("top16").cpu().numpy().astype(np.float64) * st.norm_std + 16 * st.norm_mean
-        sel = ref > np.percentile(ref, 50)  # the approximate tops are floored at 0 in normalised units
-        err[prec] = np.max(np.abs(approx[sel] - ref[sel]) / ref[sel])
+        approx = (dd.channel_array("top16").cpu().numpy().astype(np.float64) * st.norm_std
+                  + spec.num_timesteps * st.norm_mean)
+        err[prec] = float(np.max(np.abs(approx[sel] - ref[sel]) / ref[sel]))
         assert err[prec] < bound, (prec, err[prec])
-    print("max relative top-path-sum error vs FP64:", err)
+    dd.close()
+    print(json.dumps({"fp64_error_case": name, "shape": [spec.rounded_timesteps, spec.num_channels],
+                      "drift_blocks": spec.num_drift_blocks(), "max_relative_top_error": err}))
     assert err["fp32"] < 1e-6
