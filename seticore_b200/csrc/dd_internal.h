@@ -96,9 +96,6 @@ struct TreeGroup {
   int off_step;
   int elig_T1;
   float* top;
-  // Optional: only the tiles listed in tile_list[0 .. *tile_count) (device memory).
-  const int* tile_list;
-  const int* tile_count;
   // Emitting launches (tree_emit_batch): root offset r of job k at channel c goes to
   // emit_out[k * emit_job_stride + r * emit_plane_stride + c]; top is unused.
   float* emit_out;

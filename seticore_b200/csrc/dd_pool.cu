@@ -97,7 +97,7 @@ int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
   uint64_t key = fnv(1469598103934665603ull, &R, sizeof(R));
   key = fnv(key, &elem, sizeof(elem));
   for (int k = 0; k < tb.count; ++k) {
-    const int v[4] = {tb.g[k].N, tb.g[k].n_jobs, tb.g[k].tile_list ? 1 : 0, (int)tb.g[k].job_row_stride};
+    const int v[3] = {tb.g[k].N, tb.g[k].n_jobs, (int)tb.g[k].job_row_stride};
     key = fnv(key, v, sizeof(v));
   }
   auto it = p->tuned_budget.find(key);

@@ -78,6 +78,12 @@ CASES = [
     (128, 2048, 2.7939677, 2.2817014, 1.0, 3, 10),
     (256, 4096, 3.814697265625, 0.268435456, 10.0, 4, 11),
     (16, 65536, 2.7939677, 18.253611, 8.0, 8, 12),
+    # edges: fewer channels than a tile, drift ranges wider than the band, the smallest
+    # band, and more than 256 rows (a 2-row level after the 16-row level)
+    (16, 100, 2.7939677, 18.253611, 4.0, 1, 13),
+    (8, 300, 2.7939677, 18.253611, 8.0, 2, 14),
+    (2, 64, 2.7939677, 18.253611, 1.0, 1, 15),
+    (512, 2048, 3.814697265625, 0.134217728, 4.0, 3, 16),
 ]
 
 
@@ -235,3 +241,24 @@ def test_batch_equals_single_searches(torch_cuda):
         assert [(h.index, h.drift_steps, h.power, h.snr, h.coarse_channel) for h in a] == \
                [(h.index, h.drift_steps, h.power, h.snr, h.coarse_channel) for h in b]
     assert sum(len(x) for x in batch) > 70
+
+
+def test_min_drift_filter(torch_cuda, port_oracle):
+    """Hits whose |drift rate| is below min_drift are dropped (dedoppler.cu:391)."""
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    spec = SearchSpec(16, 20000, seed=41, n_tones=10, snr_threshold=8.0)
+    x = make_filterbank_numpy(spec)
+    for min_drift in (0.05, 0.5):
+        want, wstats = port_oracle.search(x, spec.foff_mhz, spec.tsamp, 4.0, min_drift, 8.0)
+        got, gstats, _, _ = run_gpu(torch_cuda, x, spec.foff_mhz, spec.tsamp, 4.0, min_drift, 8.0, T=16)
+        compare_hits(got, want, gstats.threshold, wstats["threshold"], label=f"min_drift {min_drift}")
+        assert all(abs(h["drift_rate"]) >= min_drift for h in got)
+
+
+def test_constant_input_has_no_hits(torch_cuda):
+    """Zero or constant power: every path sums to the median, nothing beats the threshold."""
+    for value in (0.0, 3.5):
+        x = np.full((16, 5000), value, dtype=np.float32)
+        got, gstats, top, _ = run_gpu(torch_cuda, x, 2.7939677e-6, 18.253611, 4.0, 0.0, 10.0, T=16)
+        assert got == []
+        assert gstats.median == np.float32(16 * value)
