@@ -304,7 +304,7 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
   EventHooks eh{dd, first_batch};
   scb::ExecHooks hooks;
   hooks.ctx = &eh;
-  hooks.after_stats = [](void* c, cudaStream_t st) {
+  hooks.before_tree = [](void* c, cudaStream_t st) {
     EventHooks* h = static_cast<EventHooks*>(c);
     if (h->record) cudaEventRecord(h->dd->ev[1], st);
   };

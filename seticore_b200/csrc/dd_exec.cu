@@ -3,9 +3,10 @@
 // Used by the engine (dd_api.cu, one shape) and by the pool (dd_pool.cu, mixed shapes).
 // The searches travel in batches of up to kMaxBatch as kernel parameters, so a call is a
 // fixed sequence of launches (capturable in a CUDA graph) whatever the mix:
-//   clear -> [normalise] -> statistics -> tree launches grouped by (rows, element type)
-//   (levels for more than 16 rows, one search at a time) -> [flag + FP32 recompute of the
-//   flagged channels] -> hits
+//   clear -> [normalise] -> column sums (searches whose tree does not compute them) ->
+//   tree launches grouped by (rows, element type), the float32 ones adding the column
+//   sums -> levels for more than 16 rows, one search at a time -> statistics ->
+//   [flag + FP32 recompute of the flagged channels] -> hits
 #include <algorithm>
 
 #include "dd_common.cuh"
@@ -15,13 +16,24 @@ namespace scb {
 
 namespace {
 
-// Zeroes, per search of the batch: top (and the 16-bit tops), the result header and the
-// flagged-channel count.
+// Zeroes, per search of the batch: top (and the 16-bit tops), the result header, the
+// radix-select state and the flagged-channel count.
 __global__ void clear_kernel(const __grid_constant__ SearchBatch b, const __grid_constant__ PrecisionBatch pb) {
   const SearchDesc& d = b.s[blockIdx.y];
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) d.top[c] = 0.0f;
   if (blockIdx.x == 0 && threadIdx.x < (int)(sizeof(SearchHeader) / 4))
     reinterpret_cast<int*>(d.hdr)[threadIdx.x] = 0;
+  if (blockIdx.x == 0) {  // the radix-select state for the three order statistics
+    SelectState* st = d.sel;
+    if (threadIdx.x < 3) {
+      const int r = threadIdx.x == 0 ? d.first : (threadIdx.x == 1 ? d.mid : d.last);
+      st->prefix[threadIdx.x] = 0;
+      st->mask[threadIdx.x] = 0;
+      st->rank[threadIdx.x] = (uint32_t)r;
+      if (threadIdx.x == 0) st->ticket = 0;
+    }
+    for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0;
+  }
   if (pb.count > 0 && blockIdx.y < (unsigned)pb.count && pb.s[blockIdx.y].flag_count) {
     const PrecisionDesc& q = pb.s[blockIdx.y];
     float* t16 = const_cast<float*>(q.top16);
@@ -77,6 +89,10 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
   q.flag_count = e.flag_count;
   return q;
 }
+
+// The float32 tree of up to 16 rows computes the search's column sums itself (its drift
+// range always holds drift block 0: dmin <= 0 <= dmax).
+bool fused_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 16 && e.dmin <= 0 && e.dmax >= 0; }
 
 TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride, float* top) {
   TreeGroup g{};
@@ -139,8 +155,20 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
         }
       if (q.count && (e = normalize_batch(q, num_sms, stream)) != cudaSuccess) return e;
     }
-    if ((e = search_stats_batch(b, num_sms, stream)) != cudaSuccess) return e;
-    if (hooks.after_stats) hooks.after_stats(hooks.ctx, stream);
+    // Column sums: the float32 trees over up to 16 rows compute their own from the staged
+    // rows; the others (16-bit forms, level path) read the input once here.
+    {
+      SearchBatch cb;
+      cb.count = 0;
+      cb.maxN = 0;
+      for (int k = 0; k < m; ++k)
+        if (!fused_colsum(ss[k])) {
+          cb.s[cb.count++] = b.s[k];
+          cb.maxN = std::max(cb.maxN, ss[k].N);
+        }
+      if ((e = column_sums_batch(cb, stream)) != cudaSuccess) return e;
+    }
+    if (hooks.before_tree) hooks.before_tree(hooks.ctx, stream);
     // Trees over up to 16 rows: one launch per (rows, element type).
     for (int R : {2, 4, 8, 16}) {
       for (int elem : {kElemF32, kElemBF16, kElemF16}) {
@@ -149,8 +177,16 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
         tb.n_items = 0;
         for (int k = 0; k < m; ++k) {
           if (ss[k].Tr != R || ss[k].elem != elem) continue;
-          if (elem == kElemF32) tb.g[tb.count++] = tree_group(ss[k], ss[k].input, ss[k].row_stride, ss[k].top);
-          else tb.g[tb.count++] = tree_group(ss[k], ss[k].norm16, ss[k].N, ss[k].top16);
+          if (elem == kElemF32) {
+            TreeGroup g = tree_group(ss[k], ss[k].input, ss[k].row_stride, ss[k].top);
+            if (fused_colsum(ss[k])) {
+              g.colsum = ss[k].colsum;
+              g.colsum_job = -ss[k].dmin;
+            }
+            tb.g[tb.count++] = g;
+          } else {
+            tb.g[tb.count++] = tree_group(ss[k], ss[k].norm16, ss[k].N, ss[k].top16);
+          }
         }
         if (tb.count && (e = tree_max_batch(tb, R, num_sms, stream, elem, hooks.budget_kb(hooks.ctx, tb, R, elem))) !=
                             cudaSuccess)
@@ -172,6 +208,8 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
                              ss[k].top, num_sms, stream, plan)) != cudaSuccess)
         return e;
     }
+    if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);
+    if ((e = search_stats_batch(b, num_sms, stream)) != cudaSuccess) return e;
     // The 16-bit searches: list the channels near the threshold, recompute them exactly
     // in FP32 from the original power.
     {
@@ -189,7 +227,6 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
         if ((e = recompute_batch(q, num_sms, stream)) != cudaSuccess) return e;
       }
     }
-    if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);
     if ((e = search_hits_batch(b, num_sms, stream)) != cudaSuccess) return e;
   }
   return cudaGetLastError();

@@ -96,6 +96,11 @@ struct TreeGroup {
   int off_step;
   int elig_T1;
   float* top;
+  // Optional column sums (sumColumns, dedoppler.cu:63-72): the CTA staging the chunk that
+  // holds job colsum_job -- the job whose shear is zero, so its window of every row covers
+  // the tile's own channels -- writes colsum[c] = x[0][c] + x[1][c] + ... in row order.
+  float* colsum;
+  int colsum_job;
   // Emitting launches (tree_emit_batch): root offset r of job k at channel c goes to
   // emit_out[k * emit_job_stride + r * emit_plane_stride + c]; top is unused.
   float* emit_out;
@@ -168,7 +173,11 @@ cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream
 // original power in the tree's pairing, the maximum floored at 0.
 cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
 
-// Column sums, order statistics, mean, standard deviation and threshold of each search.
+// Column sums of each search (searches whose tree computes them skip this); also resets
+// each search's radix-select state.
+cudaError_t column_sums_batch(const SearchBatch& b, cudaStream_t stream);
+// Order statistics, mean, standard deviation and threshold of each search, from its column
+// sums and a reset select state (column_sums_batch or exec_queue's clear launch).
 cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
 
 // Window de-duplication (dedoppler.cu:353-383) and drift recovery of the survivors.
@@ -235,7 +244,7 @@ struct ExecHooks {
   };
   // The level split of a search with more than 16 rows (may time alternatives first).
   LevelPlan (*level_plan)(void* ctx, const ExecSearch& s, float* lvl_a, float* lvl_b, cudaStream_t st) = nullptr;
-  void (*after_stats)(void* ctx, cudaStream_t s) = nullptr;
+  void (*before_tree)(void* ctx, cudaStream_t s) = nullptr;
   void (*after_tree)(void* ctx, cudaStream_t s) = nullptr;
 };
 

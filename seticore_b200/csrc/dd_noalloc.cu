@@ -156,7 +156,8 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   sd.cands = cands;
   sd.cand_cap = kStaticMaxCands;
   if (kStaticPartials < 2 * num_sms) return fail(SC_DD_EINTERNAL, "sc_dd_search_static: too many SMs for the partials");
-  if ((e = scb::search_stats_batch(batch, num_sms, stream)) != cudaSuccess)
+  if ((e = scb::column_sums_batch(batch, stream)) != cudaSuccess ||
+      (e = scb::search_stats_batch(batch, num_sms, stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: statistics kernels");
   scb::TreeBatch tb;
   tb.count = 1;

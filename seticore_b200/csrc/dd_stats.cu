@@ -28,7 +28,10 @@ namespace scb {
 
 namespace {
 
-// Column sums of search blockIdx.y; block 0 also resets that search's select state.
+constexpr int kSelectCtasPerSm = 16;
+
+// Column sums of search blockIdx.y (dedoppler.cu:63-72: a float sum in row order); block 0
+// also resets that search's select state.
 __global__ void colsum_kernel(const __grid_constant__ SearchBatch b) {
   const SearchDesc& d = b.s[blockIdx.y];
   SelectState* st = d.sel;
@@ -438,18 +441,29 @@ __global__ void var_emulate_kernel(const __grid_constant__ SearchBatch b) {
 
 }  // namespace
 
+cudaError_t column_sums_batch(const SearchBatch& b, cudaStream_t stream) {
+  if (b.count <= 0) return cudaSuccess;
+  dim3 cgrid((b.maxN + 4 * 256 - 1) / (4 * 256), b.count);
+  colsum_kernel<<<cgrid, 256, 0, stream>>>(b);
+  return cudaGetLastError();
+}
+
 cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream) {
   if (b.count <= 0) return cudaSuccess;
   const int maxN = b.maxN;
-  dim3 cgrid((maxN + 4 * 256 - 1) / (4 * 256), b.count);
-  colsum_kernel<<<cgrid, 256, 0, stream>>>(b);
   // About four CTAs per SM over the whole batch, at least 8 per search.
   int sblocks = (4 * num_sms + b.count - 1) / b.count;
   if (sblocks < 8) sblocks = 8;
   if (sblocks > 2 * num_sms) sblocks = 2 * num_sms;
   if (sblocks > (maxN + 255) / 256) sblocks = (maxN + 255) / 256;
   dim3 sgrid(sblocks, b.count);
-  for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<sgrid, 256, 0, stream>>>(b, shift);
+  // The select passes are latency-bound (a load, three warp votes and shared atomics per
+  // value): many more CTAs than the moment kernels, which need one partial per CTA.
+  int selblocks = (kSelectCtasPerSm * num_sms + b.count - 1) / b.count;
+  if (selblocks > (maxN + 255) / 256) selblocks = (maxN + 255) / 256;
+  if (selblocks < 1) selblocks = 1;
+  dim3 selgrid(selblocks, b.count);
+  for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<selgrid, 256, 0, stream>>>(b, shift);
   moments_kernel<<<sgrid, 256, 0, stream>>>(b);
   int vchunks = sblocks;
   if (vchunks > kVarChunks) vchunks = kVarChunks;

@@ -272,13 +272,32 @@ class Dedopplerer:
     def memoryUsage(self) -> int:
         return int(lib().sc_dd_memory_usage(self._h))
 
+    def _hit_buffer(self, cap: int):
+        """A reusable host array of at least `cap` hit records (allocating and zeroing a fresh
+        one per call costs milliseconds at 2^16 records)."""
+        buf = getattr(self, "_hits", None)
+        if buf is None or len(buf) < cap:
+            buf = (_capi.ScDdHit * max(cap, 1))()
+            self._hits = buf
+        return buf
+
+    @staticmethod
+    def _copy_hits(buf, start: int, count: int) -> list:
+        """Records [start, start + count) of the reusable buffer, copied out (the buffer is
+        overwritten by the next call)."""
+        out = (_capi.ScDdHit * count)()
+        if count:
+            size = ctypes.sizeof(_capi.ScDdHit)
+            ctypes.memmove(out, ctypes.addressof(buf) + start * size, count * size)
+        return list(out)
+
     def search_raw(self, input, beam: int, coarse_channel: int, max_drift: float,
                    min_drift: float, snr_threshold: float, stream=None, capacity: int = 4096):
         """Runs the search and returns the C ABI hit records (list of ScDdHit)."""
         t = _device_input(input, self.rounded_num_timesteps, self.num_channels)
         cap = capacity
         while True:
-            buf = (_capi.ScDdHit * max(cap, 1))()
+            buf = self._hit_buffer(cap)
             n = ctypes.c_int(0)
             rc = lib().sc_dd_search(self._h, ctypes.c_void_p(t.data_ptr()), t.stride(0), beam,
                                     coarse_channel, max_drift, min_drift, snr_threshold, buf, cap,
@@ -287,7 +306,7 @@ class Dedopplerer:
                 cap = n.value
                 continue
             check(rc)
-            return list(buf[: n.value])
+            return self._copy_hits(buf, 0, n.value)
 
     def search_batch_raw(self, inputs, beams, coarse_channels, max_drift: float, min_drift: float,
                          snr_threshold: float, stream=None, capacity: int = 1 << 16):
@@ -304,7 +323,7 @@ class Dedopplerer:
         counts = (ctypes.c_int * n)()
         cap = capacity
         while True:
-            buf = (_capi.ScDdHit * max(cap, 1))()
+            buf = self._hit_buffer(cap)
             rc = lib().sc_dd_search_batch(self._h, n, ptrs, strides, b, c, max_drift, min_drift, snr_threshold,
                                           buf, cap, counts, _stream_handle(stream))
             if rc == _capi.SC_DD_ETRUNC:
@@ -313,7 +332,7 @@ class Dedopplerer:
             check(rc)
             out, k = [], 0
             for cnt in counts:
-                out.append(list(buf[k:k + cnt]))
+                out.append(self._copy_hits(buf, k, cnt))
                 k += cnt
             return out
 

@@ -12,7 +12,7 @@ from typing import List, Optional
 
 from . import _capi
 from ._capi import check, lib
-from .dedoppler import _stream_handle
+from .dedoppler import Dedopplerer, _stream_handle
 
 
 @dataclass
@@ -80,7 +80,9 @@ class SearchPool:
         counts = (ctypes.c_int * n)()
         cap = capacity
         while True:
-            buf = (_capi.ScDdHit * max(cap, 1))()
+            buf = self._hits if getattr(self, "_hits", None) is not None and len(self._hits) >= cap else None
+            if buf is None:
+                buf = self._hits = (_capi.ScDdHit * max(cap, 1))()
             rc = lib().sc_dd_pool_search(self._h, reqs, n, buf, cap, counts, _stream_handle(stream))
             if rc == _capi.SC_DD_ETRUNC:
                 cap = sum(counts)
@@ -88,7 +90,7 @@ class SearchPool:
             check(rc, pool=True)
             out, k = [], 0
             for c in counts:
-                out.append(list(buf[k:k + c]))
+                out.append(Dedopplerer._copy_hits(buf, k, c))
                 k += c
             return out
 
