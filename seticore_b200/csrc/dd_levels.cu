@@ -19,6 +19,8 @@
 // default, so only the pool's autotuner, which times both per shape, may pick it.  The
 // pairing of the adds is the tree's own at every level, so every path sum is
 // bit-identical to the reference's twoStageTaylorTree (taylor.cu:298-327).
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -82,16 +84,19 @@ __global__ void emit_kernel(const float* __restrict__ src, long long src_stride,
 // M-row subtree at channel c from its 136 (M = 16) or 36 (M = 8) leaves, in the tree's
 // pairing (taylor_direct_M, generated).  Loads of neighbouring threads overlap, so most
 // come from L1; the level reads its input from HBM once and writes the planes once.
+// Problem p reads rows from src + p * src_problem_rows rows (0: every problem reads the same
+// rows, as the first level does for a chunk of drift blocks) with drift D0 + p.
 template <int M, typename E>
-__global__ void __launch_bounds__(128, 6) direct_kernel(const E* __restrict__ src, long long src_stride, int Tp,
-                                                        int D0, float* __restrict__ dst, long long dst_stride, int N) {
+__global__ void __launch_bounds__(128, 6) direct_kernel(const E* __restrict__ src, long long src_stride,
+                                                        long long src_problem_rows, int Tp, int D0,
+                                                        float* __restrict__ dst, long long dst_stride, int N) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= N) return;
   const int nb = Tp / M;
   const int p = blockIdx.y / nb;
   const int q = blockIdx.y - p * nb;
   const long long D = (long long)D0 + p;
-  const E* r0 = src + ((long long)p * Tp + (long long)q * M) * src_stride;
+  const E* r0 = src + ((long long)p * src_problem_rows + (long long)q * M) * src_stride;
   float out[M];
   // Leaves lie in [c + min(0, (M-1)D), c + (M-1) + max(0, (M-1)D)]: inside the row for
   // most channels, which then load without bounds checks.
@@ -193,26 +198,45 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
     }
     final_rows = tp;
   }
-  // scratch_b lies in the same allocation as scratch_a (the emitting level addresses both
-  // from scratch_a): job stride in floats.
-  const long long job_stride = scratch_b - scratch_a;
+  // scratch_b lies in the same allocation as scratch_a, which holds 2 * (scratch_b -
+  // scratch_a) floats: one level buffer for the ping-pong of multi-level plans, or room for
+  // the planes of several drift blocks at once.
+  const long long half = scratch_b - scratch_a;
   const long long Np = level_row_length(N);  // plane row length
+  const long long per_db = (long long)Tr * Np;
   cudaError_t err;
-  if (nlev == 1 && sizes[0] == kStreamEmit16) {
-    // Two drift blocks per pass: one staged input read emits both, one launch finishes both.
-    for (int db = dmin; db <= dmax; db += 2) {
-      const int nj = (dmax - db + 1) < 2 ? 1 : 2;
-      if ((err = emit16(input, row_stride, Tr, N, Np, db, nj, scratch_a, job_stride, num_sms, stream)) != cudaSuccess)
-        return err;
+  if (nlev == 1 && (sizes[0] == 16 || sizes[0] == kStreamEmit16)) {
+    // One level, then the last: the planes of up to J drift blocks per pair of launches.
+    long long J = 2 * half / per_db;
+    if (J > kMaxBatch) J = kMaxBatch;
+    if (J < 1) return cudaErrorInvalidValue;
+    const int nb = Tr / 16;
+    for (int db = dmin; db <= dmax; db += (int)J) {
+      const int nj = (int)std::min<long long>(J, dmax - db + 1);
+      if (sizes[0] == kStreamEmit16) {
+        if ((err = emit16(input, row_stride, Tr, N, Np, db, nj, scratch_a, per_db, num_sms, stream)) != cudaSuccess)
+          return err;
+      } else {
+        dim3 grid((N + 127) / 128, (unsigned)(nj * nb));
+        if (elem == kElemBF16)
+          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __nv_bfloat16*>(input_v), row_stride, 0, Tr, db,
+                                                     scratch_a, Np, N);
+        else if (elem == kElemF16)
+          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __half*>(input_v), row_stride, 0, Tr, db,
+                                                     scratch_a, Np, N);
+        else
+          direct_kernel<16><<<grid, 128, 0, stream>>>(input, row_stride, 0, Tr, db, scratch_a, Np, N);
+      }
       TreeBatch tb;
       tb.count = nj;
       tb.n_items = 0;
       for (int j = 0; j < nj; ++j)
-        tb.g[j] = final_group(scratch_a + j * job_stride, Np, N, final_rows, 16, 16, db + j, Tr, top);
+        tb.g[j] = final_group(scratch_a + j * per_db, Np, N, final_rows, 16, 16, db + j, Tr, top);
       if ((err = tree_max_batch(tb, final_rows, num_sms, stream)) != cudaSuccess) return err;
     }
     return cudaGetLastError();
   }
+  if (half < per_db) return cudaErrorInvalidValue;
   for (int db = dmin; db <= dmax; ++db) {
     const float* src = input;
     long long stride = row_stride;
@@ -224,18 +248,19 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
       const int D0 = (int)(dscale * db);
       if (M == kStreamEmit16) {
         M = 16;
-        if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, job_stride, num_sms, stream)) != cudaSuccess) return err;
+        if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, per_db, num_sms, stream)) != cudaSuccess) return err;
       } else if (M >= 8) {
         dim3 grid((N + 127) / 128, (unsigned)(P * (Tp / M)));
         if (l == 0 && elem == kElemBF16) {
-          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __nv_bfloat16*>(input_v), stride, Tp, D0, dst,
-                                                     Np, N);
+          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __nv_bfloat16*>(input_v), stride, Tp, Tp, D0,
+                                                     dst, Np, N);
         } else if (l == 0 && elem == kElemF16) {
-          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __half*>(input_v), stride, Tp, D0, dst, Np, N);
+          direct_kernel<16><<<grid, 128, 0, stream>>>(static_cast<const __half*>(input_v), stride, Tp, Tp, D0, dst, Np,
+                                                     N);
         } else if (M == 16) {
-          direct_kernel<16><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+          direct_kernel<16><<<grid, 128, 0, stream>>>(src, stride, Tp, Tp, D0, dst, Np, N);
         } else {
-          direct_kernel<8><<<grid, 128, 0, stream>>>(src, stride, Tp, D0, dst, Np, N);
+          direct_kernel<8><<<grid, 128, 0, stream>>>(src, stride, Tp, Tp, D0, dst, Np, N);
         }
       } else {
         dim3 grid((N + 255) / 256, (unsigned)(P * (Tp / M)));
