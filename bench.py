@@ -40,7 +40,7 @@ UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.34 MB +
 # 15.31 MB); a launch covering k coarse channels moves k times this.
-TREE_DRAM_BYTES = 75163904
+TREE_DRAM_BYTES = 78148288
 
 
 def dist_setup():

@@ -9,9 +9,11 @@
 //      order of path sums is kept up to the 16-bit rounding.
 //   4. flag_channels_kernel: lists every channel whose approximate top reaches 0.9 x the
 //      threshold in SNR units, P >= median + 0.9 * snr * std, mapped to y units.
-//   5. recompute_kernel: for each listed channel, every eligible path is summed (one path
-//      per thread) from the original power in the tree's own pairing (bit-identical to the
-//      plain form's tree) and the maximum, floored at 0, becomes its top.  Every other channel keeps top 0:
+//   5. recompute_direct_kernel (up to 16 rows: one thread per channel and drift block,
+//      all offsets from the subtree's leaves) or recompute_kernel (one path per thread):
+//      for each listed channel, every eligible path is summed from the original power in
+//      the tree's own pairing (bit-identical to the plain form's tree) and the maximum,
+//      floored at 0, becomes its top.  Every other channel keeps top 0:
 //      its approximate top is below 0.9 x threshold, so its exact top is below the
 //      threshold and it can neither become a window candidate nor beat one
 //      (dedoppler.cu:353-383 compares only with values above the threshold).  The hit list
@@ -21,6 +23,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "dd_common.cuh"
@@ -181,6 +184,42 @@ __global__ void flag_channels_kernel(const __grid_constant__ PrecisionBatch b) {
   }
 }
 
+#include "generated/taylor_direct_gen.cuh"
+
+// Up to 16 rows: one thread per (listed channel, drift block) computes all Tr in-block
+// offsets at once from the Tr-row subtree's leaves (taylor_direct_M, the tree's pairing);
+// leaves outside [0, N) read as zero, which only ineligible paths touch.
+template <int M>
+__global__ void recompute_direct_kernel(const __grid_constant__ PrecisionBatch b) {
+  const PrecisionDesc& d = b.s[blockIdx.y];
+  const long long n = *d.flag_count;
+  const int ndb = d.dmax - d.dmin + 1;
+  const int N = d.N;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n * ndb;
+       u += (long long)gridDim.x * blockDim.x) {
+    const long long k = u / ndb;
+    const int db = d.dmin + (int)(u - k * ndb);
+    const int c = d.flag_list[k];
+    const long long e = (long long)(M - 1) * db;
+    float best = 0.0f;
+    if (c + e >= 0) {  // otherwise no offset of this drift block is eligible (dedoppler.cu:40-46)
+      auto ld = [&](int t, int pos) {
+        const long long x = c + (long long)db * t + pos;
+        return (x >= 0 && x < N) ? __ldg(d.input + t * d.row_stride + x) : 0.0f;
+      };
+      float out[M];
+      if constexpr (M == 16) taylor_direct_16(ld, out);
+      else if constexpr (M == 8) taylor_direct_8(ld, out);
+      else if constexpr (M == 4) taylor_direct_4(ld, out);
+      else taylor_direct_2(ld, out);
+#pragma unroll
+      for (int off = 0; off < M; ++off)
+        if (c + e + off < N) best = fmaxf(best, out[off]);
+    }
+    if (best > 0.0f) atomicMax(reinterpret_cast<int*>(d.top) + c, __float_as_int(best));
+  }
+}
+
 // Work unit = (listed channel, block of blockDim.x of its (drift block, offset) paths),
 // one path per thread; the channel's maximum meets in global memory (atomicMax on the
 // float bits: every candidate is >= 0).
@@ -239,7 +278,28 @@ cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
   if (b.count <= 0) return cudaSuccess;
   int blocks = (16 * num_sms + b.count - 1) / b.count;
   if (blocks < 1) blocks = 1;
-  recompute_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
+  // Searches of one rounded timestep count share a launch: the direct form per row count up
+  // to 16, the per-path form beyond.
+  for (int R : {2, 4, 8, 16, 0}) {
+    PrecisionBatch q;
+    q.count = 0;
+    q.maxN = 0;
+    q.elem = b.elem;
+    for (int k = 0; k < b.count; ++k)
+      if (R ? b.s[k].Tr == R : b.s[k].Tr > 16) {
+        q.s[q.count++] = b.s[k];
+        q.maxN = std::max(q.maxN, b.s[k].N);
+      }
+    if (!q.count) continue;
+    const dim3 grid(blocks, q.count);
+    switch (R) {
+      case 2: recompute_direct_kernel<2><<<grid, 128, 0, stream>>>(q); break;
+      case 4: recompute_direct_kernel<4><<<grid, 128, 0, stream>>>(q); break;
+      case 8: recompute_direct_kernel<8><<<grid, 128, 0, stream>>>(q); break;
+      case 16: recompute_direct_kernel<16><<<grid, 128, 0, stream>>>(q); break;
+      default: recompute_kernel<<<grid, 256, 0, stream>>>(q); break;
+    }
+  }
   return cudaGetLastError();
 }
 

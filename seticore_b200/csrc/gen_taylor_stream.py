@@ -201,7 +201,7 @@ LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3),
 # (the level kernels' output planes) instead of a running maximum.
 EMIT_CONFIGS = [(16, 2, 11, 3)]
 # Subtree sizes of the one-thread-per-channel level kernel (dd_levels.cu).
-DIRECT_SIZES = [8, 16]
+DIRECT_SIZES = [2, 4, 8, 16]
 
 
 def main(out_path):
