@@ -541,7 +541,9 @@ def main():
                        "l2": "inputs (4.3 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
             "clocks": clk, "roofline": roofline, "e2e": e2e,
             "precision_forms": precision,
-            "gpu_launches": len(tree_ms) * 12 * ((n_coarse + 63) // 64),
+            # per batch of up to 64 coarse channels: clear, tree (with the column sums), four
+            # select passes, moments, two variance kernels, window and resolve
+            "gpu_launches": len(tree_ms) * 11 * ((n_coarse + 63) // 64),
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline("reference", steps=1)
