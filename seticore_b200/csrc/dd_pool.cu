@@ -92,14 +92,27 @@ struct sc_dd_pool {
 
 namespace {
 
+// Power-of-two bucket of a positive count (tuning keys describe a launch's class, not
+// its exact composition, so a mix of shapes is tuned a few times rather than per batch).
+int bucket(long long v) {
+  int b = 0;
+  while ((1ll << b) < v) ++b;
+  return b;
+}
+
 int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
   sc_dd_pool* p = static_cast<sc_dd_pool*>(ctx);
-  uint64_t key = fnv(1469598103934665603ull, &R, sizeof(R));
-  key = fnv(key, &elem, sizeof(elem));
+  // The budget decides how many drift blocks share a staged tile and how many CTAs fit an
+  // SM: the key is the rows, the element type, the largest drift-block count and the
+  // launch's total channels, each bucketed.
+  int max_jobs = 1;
+  long long channels = 0;
   for (int k = 0; k < tb.count; ++k) {
-    const int v[3] = {tb.g[k].N, tb.g[k].n_jobs, (int)tb.g[k].job_row_stride};
-    key = fnv(key, v, sizeof(v));
+    max_jobs = std::max(max_jobs, tb.g[k].n_jobs);
+    channels += tb.g[k].N;
   }
+  const int v[4] = {R, elem, bucket(max_jobs), bucket(channels)};
+  const uint64_t key = fnv(1469598103934665603ull, v, sizeof(v));
   auto it = p->tuned_budget.find(key);
   if (it != p->tuned_budget.end()) return it->second;
   if (!p->tuning || !p->tuning_now) return 0;
@@ -179,7 +192,7 @@ std::vector<scb::LevelPlan> level_candidates(int Tr) {
 
 scb::LevelPlan pool_level_plan(void* ctx, const scb::ExecSearch& s, float* la, float* lb, cudaStream_t st) {
   sc_dd_pool* p = static_cast<sc_dd_pool*>(ctx);
-  const int v[3] = {s.Tr, s.N, s.dmax - s.dmin + 1};
+  const int v[3] = {s.Tr, bucket(s.N), bucket(s.dmax - s.dmin + 1)};
   const uint64_t key = fnv(1469598103934665603ull, v, sizeof(v));
   auto it = p->tuned_plan.find(key);
   if (it != p->tuned_plan.end()) return it->second;

@@ -88,7 +88,9 @@ class SearchServer:
 
     def _work(self, stream):
         import torch
-        pool = SearchPool(scratch_budget_bytes=max(1 << 30, self.budget // 8))
+        # Arrival-time batches rarely repeat a composition, so captured graphs would seldom
+        # replay; launch shapes are still tuned per shape class on first sight.
+        pool = SearchPool(scratch_budget_bytes=max(1 << 30, self.budget // 8), cuda_graphs=False)
         while True:
             with self._cv:
                 while not self._stop and not (self._q and self._q[0].bytes <= self.budget - self.used):
