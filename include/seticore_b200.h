@@ -71,7 +71,7 @@ typedef struct sc_dd_stats {
 /* Storage of the spectra the tree reads.  FP32: the input as given (the reference's
  * form).  BF16 / FP16: each search first normalises its input per coarse channel,
  * (x - mean) / std with FP64 mean and std, into a 16-bit copy; the tree accumulates in
- * FP32 over that copy, every tile holding a channel within 0.9 x the threshold is then
+ * FP32 over that copy, every channel whose top reaches 0.9 x the threshold is then
  * recomputed in FP32 from the original power, and the hit list equals the FP32 form's. */
 enum { SC_DD_PRECISION_FP32 = 0, SC_DD_PRECISION_BF16 = 1, SC_DD_PRECISION_FP16 = 2 };
 

@@ -4,11 +4,11 @@
 // (timesteps, channels, foff, tsamp) shape and owns every scratch buffer, reused across
 // searches (dedoppler.cu:76-111).  It keeps one scratch "slot" per search of the largest
 // batch it has run.  A call queues, on the caller's stream, for up to kMaxBatch searches
-// at a time:
-//   memset(top, headers) -> column sums + order statistics + variance (dd_stats.cu)
-//   -> fused tree/top kernel over every search's work items (dd_tree.cu; for Tr > 16 the
-//      level path of dd_levels.cu, one search at a time)
-//   -> window de-duplication + drift recovery (dd_hits.cu)
+// at a time, through exec_queue (dd_exec.cu):
+//   clear -> fused tree/top kernel over every search's work items, which also forms the
+//   column sums (dd_tree.cu; for Tr > 16 the level path of dd_levels.cu, one search at a
+//   time) -> order statistics + variance (dd_stats.cu) -> window de-duplication + drift
+//   recovery (dd_hits.cu)
 // then copies the headers and the first candidates of every search to pinned host memory
 // in two copies and synchronises once.  Only hit lists cross to the host, not the
 // reference's four N-length arrays per search.

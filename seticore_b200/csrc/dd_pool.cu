@@ -7,12 +7,13 @@
 // kernel runs once for up to 64 searches, and the tree kernel's persistent CTAs pull work
 // items (tile x drift-block chunk) from all searches of the same row count.
 //
-// Autotuning: the first time a tree launch with a given composition (rows, element type,
-// the channels and drift blocks of each search) is seen, it is timed with each candidate
-// shared-memory budget (which sets how many drift blocks share a staged trapezoid and
-// how many CTAs share an SM) and the fastest is kept; likewise, each shape of more than
-// 16 rows times the candidate level splits (stage-fusion depth).  Timing reruns are
-// harmless: the tree kernel only raises per-channel maxima, so repeating it is idempotent.
+// Autotuning: the first time a tree launch of a given class (rows, element type, and the
+// power-of-two buckets of its largest drift-block count and total channels) is seen, it is
+// timed with each candidate shared-memory budget (which sets how many drift blocks share a
+// staged trapezoid and how many CTAs share an SM) and the fastest is kept; likewise, each
+// class of more than 16 rows (rows, buckets of channels and drift blocks) times the
+// candidate level splits (stage-fusion depth).  Timing reruns are harmless: the tree
+// kernel only raises per-channel maxima, so repeating it is idempotent.
 //
 // CUDA graphs: a sub-batch seen before (same requests, same arena layout) is replayed
 // from a captured graph that also holds the copies of the results to pinned host memory.
