@@ -115,6 +115,12 @@ def algorithmic_bytes_fp32(Tr, n, ndb):
     return 4 * Tr * n * (ndb + 1) + 12 * n
 
 
+def algorithmic_bytes_16bit(Tr, n, ndb):
+    """Per search of the 16-bit forms: the float32 read and 16-bit write of normalisation,
+    one 16-bit tree read per drift block and the per-channel write: 6*Tr*N + 2*Tr*N*ndb + 12*N."""
+    return 6 * Tr * n + 2 * Tr * n * ndb + 12 * n
+
+
 def cpu_baseline(kind="reference", steps=1):
     """The reference CPU Taylor path on one coarse channel of the node (bounded sample)."""
     from oracle.oracle import Oracle, available
@@ -457,7 +463,11 @@ def main():
         barrier(world)
         st = dd.last_stats()
         p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
+        alg16 = algorithmic_bytes_16bit(T, N, specs[0].num_drift_blocks()) * n_coarse
+        peak16, _ = measured_peak_hbm()
         precision[prec] = {"value": world * samples_per_step / (p_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": p_ms,
+                           "hbm_roofline_frac_of_step": alg16 / (p_ms / 1e3) / 1e9 / peak16,
+                           "algorithmic_bytes_per_step": alg16,
                            "hits_identical_to_fp32": identical,
                            "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}",
                            "speedup_vs_fp32": ms / p_ms}

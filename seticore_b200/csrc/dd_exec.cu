@@ -77,6 +77,7 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
   q.Tr = e.Tr;
   q.N = e.N;
   q.norm = e.norm16;
+  q.colsum = e.colsum;
   q.moments = e.norm_moments;
   q.ticket = e.norm_ticket;
   q.top16 = e.top16;
@@ -90,9 +91,11 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
   return q;
 }
 
-// The float32 tree of up to 16 rows computes the search's column sums itself (its drift
-// range always holds drift block 0: dmin <= 0 <= dmax).
-bool fused_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 16 && e.dmin <= 0 && e.dmax >= 0; }
+// Searches whose column sums come with another pass over the input: the float32 tree of up
+// to 16 rows (its drift range always holds drift block 0: dmin <= 0 <= dmax), and the
+// 16-bit forms' moments pass.
+bool tree_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 16 && e.dmin <= 0 && e.dmax >= 0; }
+bool fused_colsum(const ExecSearch& e) { return tree_colsum(e) || e.elem != kElemF32; }
 
 TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride, float* top) {
   TreeGroup g{};
@@ -156,7 +159,8 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       if (q.count && (e = normalize_batch(q, num_sms, stream)) != cudaSuccess) return e;
     }
     // Column sums: the float32 trees over up to 16 rows compute their own from the staged
-    // rows; the others (16-bit forms, level path) read the input once here.
+    // rows and the 16-bit forms in their moments pass; the level path reads the input once
+    // here.
     {
       SearchBatch cb;
       cb.count = 0;
@@ -179,7 +183,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
           if (ss[k].Tr != R || ss[k].elem != elem) continue;
           if (elem == kElemF32) {
             TreeGroup g = tree_group(ss[k], ss[k].input, ss[k].row_stride, ss[k].top);
-            if (fused_colsum(ss[k])) {
+            if (tree_colsum(ss[k])) {
               g.colsum = ss[k].colsum;
               g.colsum_job = -ss[k].dmin;
             }

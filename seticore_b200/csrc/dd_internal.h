@@ -149,6 +149,7 @@ struct PrecisionDesc {
   long long row_stride;
   int T, Tr, N;         // unrounded and rounded timesteps, channels
   void* norm;           // normalised 16-bit copy [Tr][N] (dense)
+  float* colsum;        // column sums of the float32 power, formed by the moments pass
   double* moments;      // 2 * kVarChunks partial sums + [mean, std] at 2 * kVarChunks
   unsigned* ticket;
   const float* top16;   // tops of the 16-bit tree (normalised units)

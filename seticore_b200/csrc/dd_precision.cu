@@ -1,7 +1,8 @@
 // The precision form: searches over normalised 16-bit spectra with exact hits.
 //
 //   1. norm_moments_kernel: per search, the FP64 mean and standard deviation of the
-//      unrounded rows of the original float32 power (zero-padded rows excluded).
+//      unrounded rows of the original float32 power (zero-padded rows excluded), and in
+//      the same read the float32 column sums the statistics need.
 //   2. normalize_kernel: y = (x - mean) / std in FP64, rounded to BF16 or FP16 (padded
 //      rows stay 0), into a dense [Tr][N] 16-bit copy -- half the bytes of the input.
 //   3. (dd_tree.cu, dd_levels.cu) the tree over y, accumulating in FP32, gives approximate
@@ -39,26 +40,41 @@ __global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
   __shared__ bool last_block;
   const long long total = (long long)d.T * d.N;
   double s1 = 0.0, s2 = 0.0;
-  // Row by row, each thread over channels (128-bit loads when the rows allow them).
+  // Each thread takes columns (four at a time with 128-bit loads when the rows allow them)
+  // down all Tr rows: the moments over the T loaded rows, and the column sums in row order
+  // as a float sum (sumColumns, dedoppler.cu:63-72, bit-identical to colsum_kernel).
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
   const bool vec = (d.N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
-  for (int t = 0; t < d.T; ++t) {
-    const float* row = d.input + (long long)t * d.row_stride;
-    if (vec) {
-      const float4* r4 = reinterpret_cast<const float4*>(row);
-      for (long long c = tid; c < d.N / 4; c += nth) {
-        const float4 v = __ldg(r4 + c);
-        const double a = v.x, b2 = v.y, c2 = v.z, e = v.w;
-        s1 += (a + b2) + (c2 + e);
-        s2 += (a * a + b2 * b2) + (c2 * c2 + e * e);
+  if (vec) {
+    for (long long c = tid; c < d.N / 4; c += nth) {
+      float4 cs = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int t = 0; t < d.Tr; ++t) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(d.input + (long long)t * d.row_stride) + c);
+        cs.x += v.x;
+        cs.y += v.y;
+        cs.z += v.z;
+        cs.w += v.w;
+        if (t < d.T) {
+          const double a = v.x, b2 = v.y, c2 = v.z, e = v.w;
+          s1 += (a + b2) + (c2 + e);
+          s2 += (a * a + b2 * b2) + (c2 * c2 + e * e);
+        }
       }
-    } else {
-      for (long long c = tid; c < d.N; c += nth) {
-        const double v = (double)__ldg(row + c);
-        s1 += v;
-        s2 += v * v;
+      if (d.colsum) reinterpret_cast<float4*>(d.colsum)[c] = cs;
+    }
+  } else {
+    for (long long c = tid; c < d.N; c += nth) {
+      float cs = 0.0f;
+      for (int t = 0; t < d.Tr; ++t) {
+        const float x = __ldg(d.input + (long long)t * d.row_stride + c);
+        cs += x;
+        if (t < d.T) {
+          s1 += (double)x;
+          s2 += (double)x * (double)x;
+        }
       }
+      if (d.colsum) d.colsum[c] = cs;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
