@@ -194,10 +194,7 @@ def gen_direct(M):
 # S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks).
 LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3),
                 # short strips (S = 11) for launches whose jobs each stage their own rows
-                (2, 1, 11, 1), (4, 1, 11, 1), (8, 1, 11, 1), (16, 2, 11, 1),
-                # 16-bit leaves: S = 66 (an odd number of 32-bit words per strip) keeps the 32
-                # lanes in distinct banks whatever the parity of the window's first element
-                (2, 1, 11, 6), (4, 1, 11, 6), (8, 1, 11, 6), (16, 2, 11, 6)]
+                (2, 1, 11, 1), (4, 1, 11, 1), (8, 1, 11, 1), (16, 2, 11, 1)]
 
 
 # (R, offset parts, U, iterations) of the emitting form: every root value goes to a sink
