@@ -192,7 +192,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
             tb.g[tb.count++] = tree_group(ss[k], ss[k].norm16, ss[k].N, ss[k].top16);
           }
         }
-        if (tb.count && (e = tree_max_batch(tb, R, num_sms, stream, elem, hooks.budget_kb(hooks.ctx, tb, R, elem))) !=
+        if (tb.count && (e = tree_max_batch(tb, R, num_sms, stream, elem, hooks.tree_launch(hooks.ctx, tb, R, elem))) !=
                             cudaSuccess)
           return e;
       }

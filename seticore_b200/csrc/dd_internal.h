@@ -118,12 +118,19 @@ struct TreeBatch {
   TreeGroup g[kMaxBatch];
 };
 
+// Launch shape of a tree launch.  smem_kb bounds the shared memory of a CTA (0: the
+// default), which sets how many drift blocks share a staged trapezoid and how many CTAs fit
+// an SM; tile is the channels per work item, 1056 or 352 (0: 1056 for jobs that share their
+// rows, 352 for jobs with their own rows).
+struct TreeLaunch {
+  int smem_kb = 0;
+  int tile = 0;
+};
+
 // Fused tree + per-channel top for the groups (all of R rows, elements of type `elem`).
-// The launcher fills the scheduling fields of `b` in place.  smem_budget_kb bounds the
-// shared memory of a CTA (0: the default), which sets how many drift blocks share a staged
-// trapezoid and how many CTAs fit an SM.
+// The launcher fills the scheduling fields of `b` in place.
 cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream, int elem = kElemF32,
-                           int smem_budget_kb = 0);
+                           TreeLaunch how = TreeLaunch{});
 
 // The same staged tree for 16 rows, writing every root value (all 16 in-block offsets of
 // every channel) to the groups' emit planes instead of folding maxima: the first level of
@@ -236,13 +243,12 @@ struct ExecSearch {
   void carve(char* base, int n_partials);
 };
 
-// Callbacks of exec_queue: the shared-memory budget of each tree launch (autotuning) and
-// points at which the caller may record events.
+// Callbacks of exec_queue: the launch shape of each tree launch (autotuning) and points at
+// which the caller may record events.
 struct ExecHooks {
   void* ctx = nullptr;
-  int (*budget_kb)(void* ctx, const TreeBatch& tb, int R, int elem) = [](void*, const TreeBatch&, int, int) {
-    return 0;
-  };
+  TreeLaunch (*tree_launch)(void* ctx, const TreeBatch& tb, int R, int elem) = [](void*, const TreeBatch&, int,
+                                                                                   int) { return TreeLaunch{}; };
   // The level split of a search with more than 16 rows (may time alternatives first).
   LevelPlan (*level_plan)(void* ctx, const ExecSearch& s, float* lvl_a, float* lvl_b, cudaStream_t st) = nullptr;
   void (*before_tree)(void* ctx, cudaStream_t s) = nullptr;

@@ -9,8 +9,9 @@
 //
 // Autotuning: the first time a tree launch of a given class (rows, element type, and the
 // power-of-two buckets of its largest drift-block count and total channels) is seen, it is
-// timed with each candidate shared-memory budget (which sets how many drift blocks share a
-// staged trapezoid and how many CTAs share an SM) and the fastest is kept; likewise, each
+// timed with each candidate launch shape -- tile width (1056 or 352 channels) and
+// shared-memory budget (which sets how many drift blocks share a staged trapezoid and how
+// many CTAs share an SM) -- and the fastest is kept; likewise, each
 // class of more than 16 rows (rows, buckets of channels and drift blocks) times the
 // candidate level splits (stage-fusion depth).  Timing reruns are harmless: the tree
 // kernel only raises per-channel maxima, so repeating it is idempotent.
@@ -83,7 +84,7 @@ struct sc_dd_pool {
   };
   std::vector<Graph> graphs;
   std::unordered_map<uint64_t, int> seen;  // sub-batch key -> times seen
-  std::unordered_map<uint64_t, int> tuned_budget;
+  std::unordered_map<uint64_t, scb::TreeLaunch> tuned_launch;
   std::unordered_map<uint64_t, scb::LevelPlan> tuned_plan;
   uint64_t clock = 0;
   int tuning = 1, use_graphs = 1;
@@ -101,11 +102,11 @@ int bucket(long long v) {
   return b;
 }
 
-int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
+scb::TreeLaunch pool_tree_launch(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
   sc_dd_pool* p = static_cast<sc_dd_pool*>(ctx);
-  // The budget decides how many drift blocks share a staged tile and how many CTAs fit an
-  // SM: the key is the rows, the element type, the largest drift-block count and the
-  // launch's total channels, each bucketed.
+  // The launch shape decides how many drift blocks share a staged tile, how wide the tile is
+  // and how many CTAs fit an SM: the key is the rows, the element type, the largest
+  // drift-block count and the launch's total channels, each bucketed.
   int max_jobs = 1;
   long long channels = 0;
   for (int k = 0; k < tb.count; ++k) {
@@ -114,15 +115,16 @@ int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
   }
   const int v[4] = {R, elem, bucket(max_jobs), bucket(channels)};
   const uint64_t key = fnv(1469598103934665603ull, v, sizeof(v));
-  auto it = p->tuned_budget.find(key);
-  if (it != p->tuned_budget.end()) return it->second;
-  if (!p->tuning || !p->tuning_now) return 0;
-  // Time each candidate budget on the stream the search runs on (idempotent reruns).
+  auto it = p->tuned_launch.find(key);
+  if (it != p->tuned_launch.end()) return it->second;
+  if (!p->tuning || !p->tuning_now) return scb::TreeLaunch{};
+  // Time each candidate on the stream the search runs on (idempotent reruns): shared-memory
+  // budgets with 1056-channel tiles, and 352-channel tiles.
   cudaStream_t s = p->cap_stream;
-  const int cands[3] = {110, 160, 200};
-  int best = 0;
+  const scb::TreeLaunch cands[5] = {{110, 1056}, {160, 1056}, {200, 1056}, {110, 352}, {48, 352}};
+  scb::TreeLaunch best{};
   float best_ms = 1e30f;
-  for (int c : cands) {
+  for (const scb::TreeLaunch& c : cands) {
     scb::TreeBatch copy = tb;
     cudaEventRecord(p->t0, s);
     if (scb::tree_max_batch(copy, R, p->num_sms, s, elem, c) != cudaSuccess) continue;
@@ -135,7 +137,7 @@ int pool_budget_kb(void* ctx, const scb::TreeBatch& tb, int R, int elem) {
       best = c;
     }
   }
-  p->tuned_budget[key] = best;
+  p->tuned_launch[key] = best;
   p->st.tuned_launches++;
   return best;
 }
@@ -269,7 +271,7 @@ cudaError_t queue_sub(sc_dd_pool* p, std::vector<Planned>& sub, cudaStream_t s) 
   for (size_t k = 0; k < sub.size(); ++k) es[k] = sub[k].es;
   scb::ExecHooks hooks;
   hooks.ctx = p;
-  hooks.budget_kb = pool_budget_kb;
+  hooks.tree_launch = pool_tree_launch;
   hooks.level_plan = pool_level_plan;
   cudaError_t e = scb::exec_queue(es.data(), (int)es.size(), p->lvl_a, p->lvl_b, p->num_sms, s, hooks);
   if (e != cudaSuccess) return e;
