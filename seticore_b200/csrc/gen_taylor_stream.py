@@ -154,11 +154,11 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
             f"    const Row (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
 
 
-def gen_direct(M):
-    """All M root values of an M-row Taylor subtree at one channel, as straight-line code:
-    every (node, position) value the roots need is computed once (bottom-up) from leaf
-    loads ld(t, pos) (row t of the block at relative channel pos; the caller applies the
-    shear).  One thread per channel, so loads and stores of a warp are coalesced."""
+def gen_direct(M, CH=1):
+    """All M root values of an M-row Taylor subtree at CH consecutive channels, as
+    straight-line code: every (node, position) value the roots need is computed once from
+    leaf loads ld(t, pos) (row t of the block at relative channel pos; the caller applies
+    the shear), so neighbouring channels share their common nodes and leaves."""
     lines = []
     done = set()
 
@@ -178,11 +178,22 @@ def gen_direct(M):
         else:
             expr = f"ld({b}, {j})"
         done.add((L, b, o, j))
-        if L == M:
+        if L == M and CH == 1:
             lines.append(f"  out[{o}] = {expr};")
         else:
             lines.append(f"  const float {nm(L, b, o, j)} = {expr};")
 
+    if CH > 1:
+        # offset-major: the CH values of one offset are complete together and go to the sink
+        # at once, so the outputs do not stay live until the end
+        for o in range(M):
+            for j in range(CH):
+                emit(M, 0, o, j)
+            args = ", ".join(nm(M, 0, o, j) for j in range(CH))
+            lines.append(f"  sink({o}, {args});")
+        body = "\n".join(lines)
+        return (f"template <typename Ld, typename Sink>\n__device__ __forceinline__ void "
+                f"taylor_direct_{M}x{CH}(const Ld& ld, const Sink& sink) {{\n{body}\n}}\n")
     for o in range(M):
         emit(M, 0, o, 0)
     body = "\n".join(lines)
@@ -202,6 +213,8 @@ LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3),
 EMIT_CONFIGS = [(16, 2, 11, 3)]
 # Subtree sizes of the one-thread-per-channel level kernel (dd_levels.cu).
 DIRECT_SIZES = [2, 4, 8, 16]
+# (rows, consecutive channels per thread) of the level kernel's multi-channel form.
+DIRECT_MULTI = [(16, 2), (16, 4)]
 
 
 def main(out_path):
@@ -238,6 +251,8 @@ def main(out_path):
     direct = ["// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n"]
     for M in DIRECT_SIZES:
         direct.append(gen_direct(M))
+    for M, CH in DIRECT_MULTI:
+        direct.append(gen_direct(M, CH))
     _write(os.path.join(os.path.dirname(out_path), "taylor_direct_gen.cuh"), "\n".join(direct))
 
 
