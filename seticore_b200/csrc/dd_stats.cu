@@ -21,6 +21,8 @@
 //     rint(t_i / ulp(float(A_i))) * ulp(float(A_i)).  The result tracks a sequential
 //     float sum to about 1e-5 relative; the remaining difference comes from the order
 //     (the reference's order is whatever std::nth_element leaves).
+#include <algorithm>
+
 #include "dd_common.cuh"
 #include "dd_internal.h"
 
@@ -465,7 +467,9 @@ cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t s
   dim3 selgrid(selblocks, b.count);
   for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<selgrid, 256, 0, stream>>>(b, shift);
   moments_kernel<<<sgrid, 256, 0, stream>>>(b);
-  int vchunks = sblocks;
+  // The variance emulation walks each chunk in 256-term tiles, one block scan per tile: short
+  // chunks (16384 channels) keep that serial walk short.
+  int vchunks = std::max(sblocks, (maxN + 16383) / 16384);
   if (vchunks > kVarChunks) vchunks = kVarChunks;
   dim3 vgrid(vchunks, b.count);
   var_chunk_kernel<<<vgrid, 256, 0, stream>>>(b);
