@@ -9,11 +9,14 @@
 //   the first (drift block, offset) in scan order whose sum beat the running maximum
 //   (dedoppler.cu:49-53); that is the first eligible path, in (drift block, offset)
 //   order, whose sum equals the final top sum.  The fused tree kernel keeps only the top
-//   value, so the few survivors recompute their paths here, bit-identically (pairwise
-//   tree order), one thread per (survivor, path); the host decodes the packed best and
-//   checks its sum against the stored top sum.
+//   value, so the few survivors recompute their paths here, bit-identically (the tree's
+//   pairing): one thread per (survivor, drift block) up to 16 rows (resolve_direct_kernel),
+//   one thread per (survivor, path) beyond; the host decodes the packed best and checks its
+//   sum against the stored top sum.
 // path_values_kernel: addIncoherentPower (dedoppler.cu:139-176): the path sum along a
 //   hit's path; the drift block is floor((float)drift_steps / (Tr-1)) in float, as there.
+#include <algorithm>
+
 #include "dd_common.cuh"
 #include "dd_internal.h"
 
@@ -115,6 +118,48 @@ __global__ void path_values_kernel(const float* __restrict__ in, long long strid
   });
 }
 
+#include "generated/taylor_direct_gen.cuh"
+
+// Up to 16 rows: one thread per (survivor, drift block) computes all Tr offsets of the
+// block from the subtree's leaves (taylor_direct_M, the tree's pairing; leaves outside
+// [0, N) read as zero, which only ineligible paths touch) and merges its best packed key.
+template <int M>
+__global__ void resolve_direct_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  const float* __restrict__ in = sd.input;
+  const long long stride = sd.row_stride;
+  const int N = sd.N, dmin = sd.dmin, ndb = sd.dmax - sd.dmin + 1, cap = sd.cand_cap;
+  Candidate* cands = sd.cands;
+  const long long n = min(sd.hdr->num_candidates, cap);
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n * ndb;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long i = idx / ndb;
+    const int j = (int)(idx - i * ndb);
+    const int db = dmin + j;
+    const long long c = cands[i].index;
+    const long long e = (long long)(M - 1) * db;
+    if (c + e < 0) continue;  // no offset of this drift block is eligible
+    auto ld = [&](int t, int pos) {
+      const long long x = c + (long long)db * t + pos;
+      return (x >= 0 && x < N) ? __ldg(in + t * stride + x) : 0.0f;
+    };
+    float out[M];
+    if constexpr (M == 16) taylor_direct_16(ld, out);
+    else if constexpr (M == 8) taylor_direct_8(ld, out);
+    else if constexpr (M == 4) taylor_direct_4(ld, out);
+    else taylor_direct_2(ld, out);
+    unsigned long long best = 0;
+#pragma unroll
+    for (int off = 0; off < M; ++off) {
+      if (c + e + off >= N || !(out[off] > 0.0f)) continue;  // eligible, and above the zero start
+      const uint32_t p = (uint32_t)(j * M + off);
+      const unsigned long long key = ((unsigned long long)float_key(out[off]) << 32) | (unsigned long long)(~p);
+      best = key > best ? key : best;
+    }
+    if (best) atomicMax(&cands[i].best, best);
+  }
+}
+
 }  // namespace
 
 cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t stream) {
@@ -131,7 +176,27 @@ cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t st
   window_kernel<<<dim3((unsigned)wblocks, b.count), 256, 0, stream>>>(b);
   int rblocks = (4 * num_sms + b.count - 1) / b.count;
   if (rblocks < 4) rblocks = 4;
-  resolve_kernel<<<dim3(rblocks, b.count), 256, 0, stream>>>(b);
+  // Drift recovery, one launch per row count: the direct form up to 16 rows, one path per
+  // thread beyond.
+  for (int R : {2, 4, 8, 16, 0}) {
+    SearchBatch q;
+    q.count = 0;
+    q.maxN = 0;
+    for (int k = 0; k < b.count; ++k)
+      if (R ? b.s[k].Tr == R : b.s[k].Tr > 16) {
+        q.s[q.count++] = b.s[k];
+        q.maxN = std::max(q.maxN, b.s[k].N);
+      }
+    if (!q.count) continue;
+    const dim3 grid(rblocks, q.count);
+    switch (R) {
+      case 2: resolve_direct_kernel<2><<<grid, 128, 0, stream>>>(q); break;
+      case 4: resolve_direct_kernel<4><<<grid, 128, 0, stream>>>(q); break;
+      case 8: resolve_direct_kernel<8><<<grid, 128, 0, stream>>>(q); break;
+      case 16: resolve_direct_kernel<16><<<grid, 128, 0, stream>>>(q); break;
+      default: resolve_kernel<<<grid, 256, 0, stream>>>(q); break;
+    }
+  }
   return cudaGetLastError();
 }
 
