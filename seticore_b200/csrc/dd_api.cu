@@ -6,7 +6,7 @@
 // batch it has run.  A call queues, on the caller's stream, for up to kMaxBatch searches
 // at a time, through exec_queue (dd_exec.cu):
 //   clear -> fused tree/top kernel over every search's work items, which also forms the
-//   column sums (dd_tree.cu; for Tr > 16 the level path of dd_levels.cu, one search at a
+//   column sums (dd_tree.cu; for Tr > 32 the level path of dd_levels.cu, one search at a
 //   time) -> order statistics + variance (dd_stats.cu) -> window de-duplication + drift
 //   recovery (dd_hits.cu)
 // then copies the headers and the first candidates of every search to pinned host memory
@@ -101,7 +101,7 @@ struct sc_dd {
   double* var = nullptr;
   scb::SearchHeader* hdrs = nullptr;
   scb::Candidate* cands = nullptr;
-  float* scratch_a = nullptr;  // Tr > 16 level buffers (one search at a time), one allocation
+  float* scratch_a = nullptr;  // Tr > 32 level buffers (one search at a time), one allocation
   float* scratch_b = nullptr;  // = scratch_a + level_buffer_floats(Tr, N)
   void* host = nullptr;  // pinned: slots * (header + kHostCands candidates)
   int* inc_index = nullptr;
@@ -453,7 +453,7 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
   d->n_partials = 2 * d->num_sms;
   // One slot; candidates for windows of 16 channels or more (grown when a call needs more).
   int rc = ensure_slots(d, 1, std::min(num_channels / 2 + 2, num_channels / 16 + 2));
-  if (rc == SC_DD_OK && d->Tr > 16) {
+  if (rc == SC_DD_OK && d->Tr > 32) {
     // Both level buffers in one allocation: the emitting level addresses them as one array.
     if ((e = dalloc(d, &d->scratch_a, 2 * sizeof(float) * scb::level_buffer_floats(d->Tr, num_channels))) !=
         cudaSuccess)

@@ -5,7 +5,7 @@
 // fixed sequence of launches (capturable in a CUDA graph) whatever the mix:
 //   clear -> [normalise] -> column sums (searches whose tree does not compute them) ->
 //   tree launches grouped by (rows, element type), the float32 ones adding the column
-//   sums -> levels for more than 16 rows, one search at a time -> statistics ->
+//   sums -> levels for more than 32 rows, one search at a time -> statistics ->
 //   [flag + FP32 recompute of the flagged channels] -> hits
 #include <algorithm>
 
@@ -92,9 +92,9 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
 }
 
 // Searches whose column sums come with another pass over the input: the float32 tree of up
-// to 16 rows (its drift range always holds drift block 0: dmin <= 0 <= dmax), and the
+// to 32 rows (its drift range always holds drift block 0: dmin <= 0 <= dmax), and the
 // 16-bit forms' moments pass.
-bool tree_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 16 && e.dmin <= 0 && e.dmax >= 0; }
+bool tree_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 32 && e.dmin <= 0 && e.dmax >= 0; }
 bool fused_colsum(const ExecSearch& e) { return tree_colsum(e) || e.elem != kElemF32; }
 
 TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride, float* top) {
@@ -158,7 +158,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
         }
       if (q.count && (e = normalize_batch(q, num_sms, stream)) != cudaSuccess) return e;
     }
-    // Column sums: the float32 trees over up to 16 rows compute their own from the staged
+    // Column sums: the float32 trees over up to 32 rows compute their own from the staged
     // rows and the 16-bit forms in their moments pass; the level path reads the input once
     // here.
     {
@@ -173,8 +173,8 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       if ((e = column_sums_batch(cb, stream)) != cudaSuccess) return e;
     }
     if (hooks.before_tree) hooks.before_tree(hooks.ctx, stream);
-    // Trees over up to 16 rows: one launch per (rows, element type).
-    for (int R : {2, 4, 8, 16}) {
+    // Trees over up to 32 rows: one launch per (rows, element type).
+    for (int R : {2, 4, 8, 16, 32}) {
       for (int elem : {kElemF32, kElemBF16, kElemF16}) {
         TreeBatch tb;
         tb.count = 0;
@@ -197,10 +197,10 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
           return e;
       }
     }
-    // More than 16 rows: the level path, one search at a time (shared level buffers); the
+    // More than 32 rows: the level path, one search at a time (shared level buffers); the
     // 16-bit searches run it on their normalised copy, with the default split.
     for (int k = 0; k < m; ++k) {
-      if (ss[k].Tr <= 16) continue;
+      if (ss[k].Tr <= 32) continue;
       if (ss[k].elem != kElemF32) {
         if ((e = levels_search(ss[k].norm16, ss[k].N, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
                                ss[k].top16, num_sms, stream, LevelPlan{}, ss[k].elem)) != cudaSuccess)

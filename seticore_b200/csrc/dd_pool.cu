@@ -416,7 +416,7 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
       i = j;
     }
     for (const Planned& pl : plans)
-      if (pl.es.Tr > 16) lvl_need = std::max(lvl_need, scb::level_buffer_floats(pl.es.Tr, pl.es.N));
+      if (pl.es.Tr > 32) lvl_need = std::max(lvl_need, scb::level_buffer_floats(pl.es.Tr, pl.es.N));
   }
   size_t host_need = 0;
   for (auto& sb : subs)
