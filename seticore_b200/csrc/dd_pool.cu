@@ -119,12 +119,17 @@ scb::TreeLaunch pool_tree_launch(void* ctx, const scb::TreeBatch& tb, int R, int
   if (it != p->tuned_launch.end()) return it->second;
   if (!p->tuning || !p->tuning_now) return scb::TreeLaunch{};
   // Time each candidate on the stream the search runs on (idempotent reruns): shared-memory
-  // budgets with 1056-channel tiles, and 352-channel tiles.
+  // budgets with 1056-channel tiles, and 352-channel tiles.  The 32-row tree runs one CTA per
+  // SM with long strips only: its candidates are the budgets from 200 KB up.
   cudaStream_t s = p->cap_stream;
-  const scb::TreeLaunch cands[5] = {{110, 1056}, {160, 1056}, {200, 1056}, {110, 352}, {48, 352}};
+  const scb::TreeLaunch cands16[5] = {{110, 1056}, {160, 1056}, {200, 1056}, {110, 352}, {48, 352}};
+  const scb::TreeLaunch cands32[2] = {{200, 1056}, {226, 1056}};
+  const scb::TreeLaunch* cands = R == 32 ? cands32 : cands16;
+  const int n_cands = R == 32 ? 2 : 5;
   scb::TreeLaunch best{};
   float best_ms = 1e30f;
-  for (const scb::TreeLaunch& c : cands) {
+  for (int ci = 0; ci < n_cands; ++ci) {
+    const scb::TreeLaunch& c = cands[ci];
     scb::TreeBatch copy = tb;
     cudaEventRecord(p->t0, s);
     if (scb::tree_max_batch(copy, R, p->num_sms, s, elem, c) != cudaSuccess) continue;

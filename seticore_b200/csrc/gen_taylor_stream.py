@@ -204,9 +204,9 @@ def gen_direct(M, CH=1):
 # (R, offset parts, U steps per iteration, iterations) compiled into the library; a strip is
 # S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks).
 LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3),
-                # 32 rows in eight parts of four offsets: a warp's part keeps its strip's
+                # 32 rows in two parts of sixteen offsets: a warp's part keeps its strip's
                 # partial sums in registers like the 16-row halves
-                (32, 8, 11, 3),
+                (32, 2, 11, 3),
                 # short strips (S = 11) for launches whose jobs each stage their own rows
                 (2, 1, 11, 1), (4, 1, 11, 1), (8, 1, 11, 1), (16, 2, 11, 1)]
 
