@@ -49,13 +49,18 @@ def lead(R, lo, hi):
     return max(max(P) for (L, b, o), P in pos.items() if L == 1)
 
 
-def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
+def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
     """Looped form: a prologue fills every node's window for step 0, then ITERS iterations
     of a U-step body; values still needed after an iteration are carried into the next
     (the loop-carried registers), and each iteration folds its U per-channel maxima into the
-    warp's row of shared memory (mrow[0..U*ITERS))."""
+    warp's row of shared memory (mrow[0..U*ITERS)).
+
+    reload > 0: leaves whose window spans `reload` positions or more are not carried; each
+    use reads the row again (a shared-memory load per use instead of a register per window
+    slot), which trades load bandwidth for registers and so for warps per SM."""
     pos = consumption(R, lo, hi)
     nodes = {k: (min(P), max(P)) for k, P in pos.items() if k[0] != R}  # (mn, lead)
+    reloaded = {k for k, (mn, ld) in nodes.items() if reload and k[0] == 1 and ld - mn >= reload}
     roots = [(R, 0, o) for o in range(lo, hi)]
 
     def nm(L, b, o):
@@ -72,7 +77,7 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
     # state arrays
     for (L, b, o) in order:
         mn, ld = nodes[(L, b, o)]
-        if ld - mn >= 1:
+        if ld - mn >= 1 and (L, b, o) not in reloaded:
             lines.append(f"  float s{nm(L, b, o)}[{ld - mn}];")
     # prologue: positions [mn, lead-1] of every node (bottom-up)
     def compute(L, b, o, j, src_pos_name):
@@ -82,12 +87,16 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
         return f"{src_pos_name(L // 2, 2 * b, o // 2, j)} + {src_pos_name(L // 2, 2 * b + 1, o // 2, j + sh)}"
 
     def prologue_name(L, b, o, j):
+        if (L, b, o) in reloaded:
+            return f"row[{b}][{j}]"
         mn, ld = nodes[(L, b, o)]
         return st(L, b, o, j - mn)
 
     # Prologue in order of position then level, so children exist before parents.
     pro = []
     for (L, b, o) in order:
+        if (L, b, o) in reloaded:
+            continue
         mn, ld = nodes[(L, b, o)]
         for j in range(mn, ld):
             pro.append((j - ld, L, f"  {prologue_name(L, b, o, j)} = {compute(L, b, o, j, prologue_name)};"))
@@ -99,6 +108,8 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
 
     # body: value names for positions j in [mn, U-1+lead] relative to iteration start
     def body_name(L, b, o, j):
+        if (L, b, o) in reloaded:
+            return f"row[{b}][base + {j}]"
         mn, ld = nodes[(L, b, o)]
         if j < ld:
             return st(L, b, o, j - mn)
@@ -106,6 +117,8 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
 
     body = []
     for (L, b, o) in order:
+        if (L, b, o) in reloaded:
+            continue
         mn, ld = nodes[(L, b, o)]
         for j in range(ld, U + ld):
             if L == 1:
@@ -140,6 +153,8 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
     # carry: new state k holds position U + mn + k
     carry = []
     for (L, b, o) in order:
+        if (L, b, o) in reloaded:
+            continue
         mn, ld = nodes[(L, b, o)]
         for k in range(ld - mn):
             carry.append(f"    {st(L, b, o, k)} = {body_name(L, b, o, U + mn + k)};")
@@ -150,8 +165,12 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False):
         return (f"template <typename Row, typename Sink>\n"
                 f"__device__ __forceinline__ void taylor_strip_emit_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
                 f"    const Row (&row)[{R}], Sink& sink) {{\n{body_text}\n}}\n")
-    return (f"template <typename Row>\n__device__ __forceinline__ void taylor_strip_loop_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
+    return (f"template <typename Row>\n__device__ __forceinline__ void {loop_name(R, lo, hi, U, ITERS, reload)}(\n"
             f"    const Row (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
+
+
+def loop_name(R, lo, hi, U, ITERS, reload=0):
+    return f"taylor_strip_loop_{R}_{lo}_{hi}_{U}_{ITERS}" + (f"_r{reload}" if reload else "")
 
 
 def gen_direct(M, CH=1):
@@ -201,11 +220,11 @@ def gen_direct(M, CH=1):
             f"float (&out)[{M}]) {{\n{body}\n}}\n")
 
 
-# (R, offset parts, U steps per iteration, iterations) compiled into the library; a strip is
-# S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks).
-LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 2, 11, 3),
-                # 32 rows in two parts of sixteen offsets: a warp's part keeps its strip's
-                # partial sums in registers like the 16-row halves
+# (R, offset parts, U steps per iteration, iterations[, reload]) compiled into the library; a
+# strip is S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks);
+# reload: leaves with windows of that many positions or more are read again at each use.
+LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 1, 11, 3),
+                # 32 rows in two parts of sixteen offsets
                 (32, 2, 11, 3),
                 # short strips (S = 11) for launches whose jobs each stage their own rows
                 (2, 1, 11, 1), (4, 1, 11, 1), (8, 1, 11, 1), (16, 2, 11, 1)]
@@ -222,24 +241,25 @@ DIRECT_MULTI = [(16, 2), (16, 4)]
 
 def main(out_path):
     parts = ["// GENERATED by gen_taylor_stream.py -- do not edit.\n#pragma once\n"]
-    for R, nparts, U, IT in LOOP_CONFIGS:
+    for R, nparts, U, IT, *rl in LOOP_CONFIGS:
         step = R // nparts
         for k in range(nparts):
-            parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT))
+            parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, reload=rl[0] if rl else 0))
     for R, nparts, U, IT in EMIT_CONFIGS:
         step = R // nparts
         for k in range(nparts):
             parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, emit=True))
 
-    # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS>(row, mrow) for any element accessor.
-    parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row>\n"
+    # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS, RELOAD>(row, mrow) for any element accessor.
+    parts.append("template <int R, int LO, int HI, int U, int ITERS, int RELOAD = 0, typename Row>\n"
                  "__device__ __forceinline__ void taylor_strip_loop(const Row (&row)[R], float* __restrict__ mrow) {")
-    for R, nparts, U, IT in LOOP_CONFIGS:
+    for R, nparts, U, IT, *rl in LOOP_CONFIGS:
         step = R // nparts
+        rel = rl[0] if rl else 0
         for k in range(nparts):
             lo, hi = k * step, (k + 1) * step
-            parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT}) "
-                         f"taylor_strip_loop_{R}_{lo}_{hi}_{U}_{IT}(row, mrow);")
+            parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT} && "
+                         f"RELOAD == {rel}) {loop_name(R, lo, hi, U, IT, rel)}(row, mrow);")
     parts.append("}")
     parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row, typename Sink>\n"
                  "__device__ __forceinline__ void taylor_strip_emit(const Row (&row)[R], Sink& sink) {")
