@@ -538,7 +538,7 @@ def main():
     achieved = alg / (tree_launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (TREE_DRAM_BYTES * per_launch if TREE_DRAM_BYTES else None), "peak_source": peak_src,
-                "kernel": "tree_max_kernel<float,16,1,33> (4 warps, 2 CTAs per SM)", "searches_per_launch": per_launch,
+                "kernel": "tree_max_kernel<float,16,1,33> (8 warps, 2 CTAs per SM, leaves reloaded from 8)", "searches_per_launch": per_launch,
                 "kernel_ms": tree_launch_ms, "algorithmic_bytes_per_launch": alg,
                 "note": "algorithmic bytes assume one tree read per drift block; the fused kernel stages each "
                         "input tile once for all drift blocks, so frac > 1 is expected"}
