@@ -226,7 +226,7 @@ const char* sc_dd_pool_last_error(void);
  * Same inputs, results and ordering as sc_dd_search, plus the shape (unrounded
  * num_timesteps, num_channels, foff in MHz, tsamp in s) that sc_dd_create would take.
  * It calls no cudaMalloc, cudaFree, cudaMallocHost or other allocating routine: its scratch
- * is one fixed device array inside the library (about 9.2 MB, held by every GPU that loads
+ * is one fixed device array inside the library (about 10.1 MB, held by every GPU that loads
  * the library until the process exits) and its host side uses the stack and `out`.
  * Limits (SC_DD_ELIMIT beyond them): num_channels <= SC_DD_STATIC_MAX_CHANNELS, rounded
  * timesteps <= 16, at most 65536 windows (num_channels / window_size).  Errors are status

@@ -63,6 +63,10 @@ __device__ __forceinline__ float key_float(uint32_t k) {
   return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
+// Key of the order statistics: -0 is keyed as +0, so that key order is float order and
+// equal floats have equal keys (for every non-NaN value).
+__device__ __forceinline__ uint32_t sel_key(float f) { return float_key(f == 0.0f ? 0.0f : f); }
+
 // Floor division for possibly negative numerators, positive divisor.
 __host__ __device__ __forceinline__ long long floor_div(long long a, long long b) {
   return (a >= 0) ? a / b : -((-a + b - 1) / b);

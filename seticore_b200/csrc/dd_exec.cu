@@ -17,23 +17,13 @@ namespace scb {
 namespace {
 
 // Zeroes, per search of the batch: top (and the 16-bit tops), the result header, the
-// radix-select state and the flagged-channel count.
+// order-statistic state and the flagged-channel count.
 __global__ void clear_kernel(const __grid_constant__ SearchBatch b, const __grid_constant__ PrecisionBatch pb) {
   const SearchDesc& d = b.s[blockIdx.y];
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) d.top[c] = 0.0f;
   if (blockIdx.x == 0 && threadIdx.x < (int)(sizeof(SearchHeader) / 4))
     reinterpret_cast<int*>(d.hdr)[threadIdx.x] = 0;
-  if (blockIdx.x == 0) {  // the radix-select state for the three order statistics
-    SelectState* st = d.sel;
-    if (threadIdx.x < 3) {
-      const int r = threadIdx.x == 0 ? d.first : (threadIdx.x == 1 ? d.mid : d.last);
-      st->prefix[threadIdx.x] = 0;
-      st->mask[threadIdx.x] = 0;
-      st->rank[threadIdx.x] = (uint32_t)r;
-      if (threadIdx.x == 0) st->ticket = 0;
-    }
-    for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0;
-  }
+  if (blockIdx.x == 0) reset_select(d.sel, d.first, d.mid, d.last);  // the order-statistic state
   if (pb.count > 0 && blockIdx.y < (unsigned)pb.count && pb.s[blockIdx.y].flag_count) {
     const PrecisionDesc& q = pb.s[blockIdx.y];
     float* t16 = const_cast<float*>(q.top16);

@@ -15,18 +15,52 @@ constexpr int kElemF32 = 0;
 constexpr int kElemBF16 = 1;
 constexpr int kElemF16 = 2;
 
-// Radix-select state for the three column-sum order statistics (first, mid, last).
+constexpr int kSelBins = 4096;   // histogram bins per order-statistic pass
+constexpr int kSelCands = 4096;  // candidates kept per order statistic for the exact pick
+
+// Order-statistic state for the three column-sum ranks (first, mid, last).  Each target's
+// key range narrows by histogram passes until it holds one key (mode 2) or at most kSelCands
+// values (mode 1), which a compaction pass collects for an exact pick.  Keys are the
+// order-preserving unsigned images of the floats (sel_key: -0 keyed as +0).
 struct SelectState {
-  uint32_t prefix[3];
-  uint32_t mask[3];
-  uint32_t rank[3];
+  uint32_t prefix[3];  // the selected keys, once known (read by the variance kernels)
+  uint32_t lo[3];      // current range of each target: [lo, lo + 2^wshift)
+  uint32_t wshift[3];
+  uint32_t rank[3];    // rank of the target inside its range
+  uint32_t count[3];   // values inside the range
+  uint32_t mode[3];    // 0: narrow further, 1: pick from candidates, 2: exact (one key)
+  uint32_t ncand[3];
+  uint32_t kmin, kmax;
   unsigned ticket;
-  unsigned hist[3][256];
-  // filled by moments_kernel for the variance kernels
+  // filled by the order-statistic finaliser for the variance kernels
   float mean;
   int pad;
   long long n_lo, n_hi, n;
+  unsigned hist[3][kSelBins];
+  uint32_t cand[3][kSelCands];
 };
+
+#ifdef __CUDACC__
+// Resets the order-statistic state of one search; run by every thread of one block.
+__device__ __forceinline__ void reset_select(SelectState* st, int first, int mid, int last) {
+  if (threadIdx.x < 3) {
+    const int j = threadIdx.x;
+    st->prefix[j] = 0;
+    st->lo[j] = 0;
+    st->wshift[j] = 0;
+    st->rank[j] = (uint32_t)(j == 0 ? first : (j == 1 ? mid : last));
+    st->count[j] = 0;
+    st->mode[j] = 0;
+    st->ncand[j] = 0;
+  }
+  if (threadIdx.x == 0) {
+    st->kmin = 0xffffffffu;
+    st->kmax = 0u;
+    st->ticket = 0;
+  }
+  for (int i = threadIdx.x; i < 3 * kSelBins; i += blockDim.x) (&st->hist[0][0])[i] = 0;
+}
+#endif
 
 struct MomentPartial {
   double s1, s2;  // s2 unused (kept for layout)

@@ -4,12 +4,15 @@
 // median and the 5% / 95% order statistics, then a mean and standard deviation over the
 // sorted positions [ceil(0.05 N), floor(0.95 N)] (dedoppler.cu:322-342).  Here:
 //   * colsum_kernel: sumColumns (dedoppler.cu:63-72), same sequential float order.
-//   * select_pass (x4): MSB-first radix select of the three order statistics at once,
-//     8 bits per pass; the last CTA of each pass picks the digits.  Exact.
-//   * moments_kernel: the sum (FP64, as the reference's std::accumulate with a double
-//     start) of the values between the two percentiles, with boundary ties counted
-//     exactly; per-CTA partials are combined by the last CTA in a fixed order.  It forms
-//     the mean with the reference's roundings (float sum, float division).
+//   * range_kernel, hist_kernel (x3), compact_kernel, select_finish_kernel: the three order
+//     statistics at once.  The key range [kmin, kmax] is cut into 4096 bins; the bin holding
+//     each target rank becomes that target's range, and further passes cut it again until
+//     the range is one key or holds at most 4096 values, which are then collected and
+//     sorted in shared memory.  Exact, and typically two reads of the column sums after the
+//     range: one histogram and the compaction.  The compaction also sums (FP64, as the
+//     reference's std::accumulate with a double start) the values between the two
+//     percentiles' ranges; the finaliser adds the boundary candidates and ties exactly and
+//     forms the mean with the reference's roundings (float sum, float division).
 //   * var_chunk_kernel + var_emulate_kernel: the variance.  The reference accumulates
 //     (f - m)^2 in FLOAT, one term at a time (dedoppler.cu:337-341).  Once the
 //     accumulator is large, every term is rounded to the accumulator's ulp and terms
@@ -30,23 +33,14 @@ namespace scb {
 
 namespace {
 
-constexpr int kSelectCtasPerSm = 16;
+constexpr int kSelThreads = 512;   // histogram and finaliser blocks
 
 // Column sums of search blockIdx.y (dedoppler.cu:63-72: a float sum in row order); block 0
 // also resets that search's select state.
 __global__ void colsum_kernel(const __grid_constant__ SearchBatch b) {
   const SearchDesc& d = b.s[blockIdx.y];
   SelectState* st = d.sel;
-  if (blockIdx.x == 0) {
-    if (threadIdx.x < 3) {
-      const int r = threadIdx.x == 0 ? d.first : (threadIdx.x == 1 ? d.mid : d.last);
-      st->prefix[threadIdx.x] = 0;
-      st->mask[threadIdx.x] = 0;
-      st->rank[threadIdx.x] = (uint32_t)r;
-      if (threadIdx.x == 0) st->ticket = 0;
-    }
-    for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0;
-  }
+  if (blockIdx.x == 0) reset_select(st, d.first, d.mid, d.last);
   const float* in = d.input;
   const long long row_stride = d.row_stride;
   const int N = d.N, Tr = d.Tr;
@@ -77,82 +71,129 @@ __global__ void colsum_kernel(const __grid_constant__ SearchBatch b) {
 // the same digit (common for the leading digits: neighbouring channels have similar sums)
 // one atomic adds them all; otherwise each lane adds to its warp's private histogram, so
 // only lanes of one warp with equal digits contend.
-__device__ __forceinline__ void warp_hist_add(unsigned* hist, uint32_t d, bool pred) {
-  const unsigned active = __ballot_sync(0xffffffffu, pred);
-  if (active == 0u) return;
-  const int first = __ffs(active) - 1;
-  const uint32_t d0 = __shfl_sync(0xffffffffu, d, first);
-  const bool same = __all_sync(0xffffffffu, !pred || d == d0);
-  if (same) {
-    if ((int)(threadIdx.x & 31) == first) atomicAdd(&hist[d0], (unsigned)__popc(active));
-  } else if (pred) {
-    atomicAdd(&hist[d], 1u);
-  }
-}
-
-// Picks, for each target, the digit whose cumulative count passes its rank: 256 threads
-// scan the 256 bins in parallel.
-__device__ void select_digits(SelectState* st, int shift) {
-  __shared__ unsigned cnt[256];
-  __shared__ unsigned incl[256];
-  for (int j = 0; j < 3; ++j) {
-    const int d = threadIdx.x;
-    const uint32_t rank = st->rank[j];  // read before any thread can update it below
-    if (d < 256) cnt[d] = __ldcg(&st->hist[j][d]);
-    __syncthreads();
-    if (d < 256) {
-      unsigned v = cnt[d];
-      // inclusive scan over 256 bins (8 warps x 32) via shared memory doubling
-      incl[d] = v;
-    }
-    __syncthreads();
-    for (int o = 1; o < 256; o <<= 1) {
-      unsigned add = 0;
-      if (d < 256 && d >= o) add = incl[d - o];
-      __syncthreads();
-      if (d < 256) incl[d] += add;
-      __syncthreads();
-    }
-    if (d < 256) {
-      const unsigned before = incl[d] - cnt[d];
-      if (rank >= before && rank < incl[d]) {
-        st->rank[j] = rank - before;
-        st->prefix[j] |= (uint32_t)d << shift;
-        st->mask[j] |= 255u << shift;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// One 8-bit radix-select pass for the three target ranks.
-__global__ void __launch_bounds__(256) select_pass(const __grid_constant__ SearchBatch b, int shift) {
-  const SearchDesc& sd = b.s[blockIdx.y];
-  const float* __restrict__ x = sd.colsum;
-  const int N = sd.N;
-  SelectState* st = sd.sel;
-  __shared__ unsigned whist[8][3][256];  // one histogram per warp
-  __shared__ bool last_block;
-  for (int i = threadIdx.x; i < 8 * 3 * 256; i += blockDim.x) (&whist[0][0][0])[i] = 0;
-  __syncthreads();
-  unsigned (*hist)[256] = whist[threadIdx.x >> 5];
-  const uint32_t p0 = st->prefix[0], p1 = st->prefix[1], p2 = st->prefix[2];
-  const uint32_t m0 = st->mask[0], m1 = st->mask[1], m2 = st->mask[2];
+// Visits the column sums of one search, four at a time where the array allows, with every
+// lane of a warp running the same trip count (for warp-wide votes inside fn).
+template <typename Fn>
+__device__ __forceinline__ void for_each_colsum(const float* __restrict__ x, int N, Fn fn) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int stride = gridDim.x * blockDim.x;
-  const int n_round = ((N + stride - 1) / stride) * stride;  // every lane runs the same trip count
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
-    const bool in = i < N;
-    const uint32_t k = in ? float_key(x[i]) : 0u;
-    const uint32_t d = (k >> shift) & 255u;
-    warp_hist_add(hist[0], d, in && (k & m0) == p0);
-    warp_hist_add(hist[1], d, in && (k & m1) == p1);
-    warp_hist_add(hist[2], d, in && (k & m2) == p2);
+  const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+  const int n4 = vec ? N / 4 : 0;
+  const int r4 = (n4 + stride - 1) / stride * stride;
+  for (int i = tid; i < r4; i += stride) {
+    const bool in = i < n4;
+    const float4 v = in ? __ldg(reinterpret_cast<const float4*>(x) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    fn(v.x, in);
+    fn(v.y, in);
+    fn(v.z, in);
+    fn(v.w, in);
+  }
+  const int rest = N - 4 * n4;
+  const int rr = (rest + stride - 1) / stride * stride;
+  for (int i = tid; i < rr; i += stride) {
+    const bool in = i < rest;
+    fn(in ? x[4 * n4 + i] : 0.0f, in);
+  }
+}
+
+// The smallest and largest key of each search's column sums.
+__global__ void __launch_bounds__(256) range_kernel(const __grid_constant__ SearchBatch b) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  uint32_t kmn = 0xffffffffu, kmx = 0u;
+  for_each_colsum(sd.colsum, sd.N, [&](float f, bool in) {
+    if (in) {
+      const uint32_t k = sel_key(f);
+      kmn = min(kmn, k);
+      kmx = max(kmx, k);
+    }
+  });
+  kmn = __reduce_min_sync(0xffffffffu, kmn);
+  kmx = __reduce_max_sync(0xffffffffu, kmx);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&sd.sel->kmin, kmn);
+    atomicMax(&sd.sel->kmax, kmx);
+  }
+}
+
+// Number of bits that hold v (0 for 0).
+__device__ __forceinline__ uint32_t bit_width(uint32_t v) { return 32u - (uint32_t)__clz((int)v); }
+
+// One histogram pass of the order statistics.  Pass 0 bins the whole key range of the search
+// ([kmin, kmax], one histogram for the three targets); later passes bin, for each target
+// still in mode 0, the range its previous pass chose.  The last CTA of the search picks each
+// active target's bin and updates its range, rank and mode.  Exact: the ranges nest, and
+// a range of width one is the target's key.
+__global__ void __launch_bounds__(kSelThreads) hist_kernel(const __grid_constant__ SearchBatch b, int pass) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  SelectState* st = sd.sel;
+  const int N = sd.N;
+  extern __shared__ unsigned sh_hist[];  // [slots][kSelBins]
+  __shared__ uint32_t s_lo[3], s_ws[3];
+  __shared__ int s_slot[3];
+  __shared__ int s_slots;
+  __shared__ bool last_block;
+  if (threadIdx.x == 0) {
+    int slots = 0;
+    for (int j = 0; j < 3; ++j) {
+      s_slot[j] = -1;
+      uint32_t lo, ws;
+      bool active;
+      if (pass == 0) {
+        lo = st->kmin;
+        ws = bit_width(st->kmax - st->kmin);  // the range [kmin, kmin + 2^ws) holds kmax
+        active = N > 0;
+      } else {
+        lo = st->lo[j];
+        ws = st->wshift[j];
+        active = st->mode[j] == 0 && N > 0;
+      }
+      s_lo[j] = lo;
+      s_ws[j] = ws;
+      if (!active) continue;
+      for (int i = 0; i < j; ++i)  // targets with the same range share a histogram
+        if (s_slot[i] >= 0 && s_lo[i] == lo && s_ws[i] == ws) s_slot[j] = s_slot[i];
+      if (s_slot[j] < 0) s_slot[j] = slots++;
+    }
+    s_slots = slots;
   }
   __syncthreads();
-  const int nw = blockDim.x >> 5;
-  for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) {
-    unsigned v = 0;
-    for (int w = 0; w < nw; ++w) v += (&whist[w][0][0])[i];
+  const int slots = s_slots;
+  if (slots == 0) return;  // every target is resolved or collected: nothing to bin
+  for (int i = threadIdx.x; i < slots * kSelBins; i += blockDim.x) sh_hist[i] = 0;
+  uint32_t lo[3], bs[3];
+  unsigned long long width[3];
+  int slot_of[3];
+  int first_of_slot[3] = {-1, -1, -1};
+  for (int j = 0; j < 3; ++j) {
+    lo[j] = s_lo[j];
+    width[j] = 1ull << s_ws[j];
+    bs[j] = s_ws[j] > 12u ? s_ws[j] - 12u : 0u;  // 2^bs keys per bin: at most kSelBins bins
+    slot_of[j] = s_slot[j];
+    if (slot_of[j] >= 0 && first_of_slot[slot_of[j]] < 0) first_of_slot[slot_of[j]] = j;
+  }
+  // Per-slot range, in registers for the loop below (s is a constant there).
+  uint32_t slo[3] = {0u, 0u, 0u}, sbs[3] = {0u, 0u, 0u};
+  unsigned long long swidth[3] = {0ull, 0ull, 0ull};
+  for (int s = 0; s < 3; ++s) {
+    const int j = first_of_slot[s];
+    if (j < 0) continue;
+    slo[s] = lo[j];
+    sbs[s] = bs[j];
+    swidth[s] = width[j];  // 0 for unused slots: nothing is binned there
+  }
+  __syncthreads();
+  for_each_colsum(sd.colsum, N, [&](float f, bool in) {
+    if (!in) return;
+    const uint32_t k = sel_key(f);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const uint32_t d = k - slo[s];
+      if (k >= slo[s] && (unsigned long long)d < swidth[s]) atomicAdd(&sh_hist[s * kSelBins + (d >> sbs[s])], 1u);
+    }
+  });
+  __syncthreads();
+  for (int i = threadIdx.x; i < slots * kSelBins; i += blockDim.x) {
+    const unsigned v = sh_hist[i];
     if (v) atomicAdd(&st->hist[0][0] + i, v);
   }
   __threadfence();
@@ -161,104 +202,220 @@ __global__ void __launch_bounds__(256) select_pass(const __grid_constant__ Searc
   __syncthreads();
   if (!last_block) return;
   __threadfence();
-  // The last CTA: choose each target's digit, then clear the histogram for the next pass.
-  select_digits(st, shift);
-  for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0;
+  // The last CTA: for each active target, the bin that holds its rank.  Thread t owns bins
+  // [t * per, (t + 1) * per) of the slot; a block scan of the per-thread totals places them.
+  constexpr int per = kSelBins / kSelThreads;
+  __shared__ unsigned warp_sum[kSelThreads / 32];
+  for (int j = 0; j < 3; ++j) {
+    const int s = slot_of[j];
+    if (s < 0) continue;
+    const unsigned* h = st->hist[s];
+    unsigned c[per];
+    unsigned tot = 0;
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+      c[q] = __ldcg(h + threadIdx.x * per + q);
+      tot += c[q];
+    }
+    // exclusive scan of tot over the block
+    unsigned inc = tot;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_sum[warp] = inc;
+    __syncthreads();
+    unsigned before = 0;
+    for (int w = 0; w < warp; ++w) before += warp_sum[w];
+    before += inc - tot;
+    const uint32_t rank = st->rank[j];  // every thread reads it before the owner updates it
+    __syncthreads();
+    if (rank >= before && rank < before + tot) {
+      unsigned acc = before;
+      for (int q = 0; q < per; ++q) {
+        if (rank < acc + c[q]) {
+          const uint32_t bin = (uint32_t)(threadIdx.x * per + q);
+          const uint32_t nlo = lo[j] + (bin << bs[j]);
+          st->lo[j] = nlo;
+          st->wshift[j] = bs[j];
+          st->rank[j] = rank - acc;
+          st->count[j] = c[q];
+          const uint32_t mode = bs[j] == 0 ? 2u : (c[q] <= (unsigned)kSelCands ? 1u : 0u);
+          st->mode[j] = mode;
+          if (mode == 2) st->prefix[j] = nlo;
+          break;
+        }
+        acc += c[q];
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < slots * kSelBins; i += blockDim.x) (&st->hist[0][0])[i] = 0;
   if (threadIdx.x == 0) st->ticket = 0;
 }
 
-__global__ void moments_kernel(const __grid_constant__ SearchBatch b) {
+// Collects the values of each mode-1 target's range (at most kSelCands each) and sums, in
+// FP64, the values strictly between the first and the last target's ranges: the part of the
+// 5-95 % mean that needs no exact boundary.  One partial per CTA.
+__global__ void __launch_bounds__(256) compact_kernel(const __grid_constant__ SearchBatch b) {
   const SearchDesc& sd = b.s[blockIdx.y];
-  const float* __restrict__ x = sd.colsum;
-  const int N = sd.N;
   SelectState* st = sd.sel;
-  const int first = sd.first, last = sd.last;
-  MomentPartial* partials = sd.partials;
-  SearchHeader* hdr = sd.hdr;
-  __shared__ MomentPartial red[32];
-  __shared__ bool last_block;
-  const float v_first = key_float(st->prefix[0]);
-  const float v_mid = key_float(st->prefix[1]);
-  const float v_last = key_float(st->prefix[2]);
-  MomentPartial acc = {0.0, 0.0, 0ull, 0ull, 0ull, 0ull};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const float f = x[i];
-    if (f > v_first && f < v_last) {
-      acc.s1 += (double)f;
+  __shared__ double red[8];
+  uint32_t lo[3], mode[3];
+  unsigned long long width[3];
+  for (int j = 0; j < 3; ++j) {
+    lo[j] = st->lo[j];
+    width[j] = 1ull << st->wshift[j];
+    mode[j] = st->mode[j];
+  }
+  // The ranges of two targets are equal or disjoint (they refine the same bins).  Interior:
+  // keys above the first target's range and below the last's.
+  const bool disjoint = lo[0] != lo[2];
+  const unsigned long long in_lo = (unsigned long long)lo[0] + width[0];
+  const uint32_t in_hi = lo[2];
+  const int lane = threadIdx.x & 31;
+  double acc = 0.0;
+  for_each_colsum(sd.colsum, sd.N, [&](float f, bool in) {
+    const uint32_t k = sel_key(f);
+    if (in && disjoint && (unsigned long long)k >= in_lo && k < in_hi) acc += (double)f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if (mode[j] != 1) continue;
+      const bool take = in && k >= lo[j] && (unsigned long long)(k - lo[j]) < width[j];
+      const unsigned m = __ballot_sync(0xffffffffu, take);
+      if (m == 0) continue;
+      const int leader = __ffs(m) - 1;
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(&st->ncand[j], (unsigned)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (take) {
+        const unsigned at = base + (unsigned)__popc(m & ((1u << lane) - 1u));
+        if (at < (unsigned)kSelCands) st->cand[j][at] = k;
+      }
     }
-    acc.lt_first += (f < v_first);
-    acc.eq_first += (f == v_first);
-    acc.lt_last += (f < v_last);
-    acc.eq_last += (f == v_last);
-  }
-  // Warp then block reduction in a fixed order.
-  for (int o = 16; o > 0; o >>= 1) {
-    acc.s1 += __shfl_down_sync(0xffffffffu, acc.s1, o);
-    acc.lt_first += __shfl_down_sync(0xffffffffu, acc.lt_first, o);
-    acc.eq_first += __shfl_down_sync(0xffffffffu, acc.eq_first, o);
-    acc.lt_last += __shfl_down_sync(0xffffffffu, acc.lt_last, o);
-    acc.eq_last += __shfl_down_sync(0xffffffffu, acc.eq_last, o);
-  }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) red[warp] = acc;
+  });
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
-    MomentPartial b = red[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-      b.s1 += red[w].s1;
-      b.lt_first += red[w].lt_first;
-      b.eq_first += red[w].eq_first;
-      b.lt_last += red[w].lt_last;
-      b.eq_last += red[w].eq_last;
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    MomentPartial mp{};
+    mp.s1 = t;
+    sd.partials[blockIdx.x] = mp;
+  }
+}
+
+// Sorts n (<= kSelCands) keys in shared memory, ascending (bitonic, padded with the largest
+// key).
+__device__ void sort_keys(uint32_t* k, int n) {
+  int p = 1;
+  while (p < n) p <<= 1;
+  for (int i = n + threadIdx.x; i < p; i += blockDim.x) k[i] = 0xffffffffu;
+  __syncthreads();
+  for (int size = 2; size <= p; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < p / 2; i += blockDim.x) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const uint32_t a = k[lo], c = k[hi];
+        if ((a > c) == up) {
+          k[lo] = c;
+          k[hi] = a;
+        }
+      }
+      __syncthreads();
     }
-    partials[blockIdx.x] = b;
-    __threadfence();
-    last_block = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
+  }
+}
+
+// One CTA per search: the exact order statistics from the collected candidates, then the
+// mean over the sorted positions [first, last] as the reference forms it (dedoppler.cu:322-336):
+// a double sum of the floats, rounded to float, divided by the count in float.
+__global__ void __launch_bounds__(kSelThreads) select_finish_kernel(const __grid_constant__ SearchBatch b,
+                                                                    int n_partials) {
+  const SearchDesc& sd = b.s[blockIdx.y];
+  SelectState* st = sd.sel;
+  SearchHeader* hdr = sd.hdr;
+  __shared__ uint32_t keys[kSelCands];
+  __shared__ uint32_t s_key[3];
+  __shared__ long long s_lt[3], s_eq[3];
+  __shared__ double red[kSelThreads / 32];
+  if (sd.N <= 0) return;
+  const int ranks[3] = {sd.first, sd.mid, sd.last};
+  for (int j = 0; j < 3; ++j) {
+    const uint32_t mode = st->mode[j];
+    const uint32_t rank = st->rank[j];
+    const long long below = (long long)ranks[j] - rank;  // values under the target's range
+    if (mode == 2) {
+      if (threadIdx.x == 0) {
+        s_key[j] = st->prefix[j];
+        s_lt[j] = below;
+        s_eq[j] = st->count[j];
+      }
+      continue;
+    }
+    // mode 1: exactly count[j] candidates were collected
+    const int n = (int)min(st->ncand[j], (unsigned)kSelCands);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) keys[i] = __ldcg(&st->cand[j][i]);
+    __syncthreads();
+    sort_keys(keys, n);
+    // The rank is below the range's count, which is the number collected; the clamp only
+    // keeps the read inside the array.
+    const int r = n > 0 ? min((int)rank, n - 1) : 0;
+    const uint32_t key = n > 0 ? keys[r] : st->lo[j];
+    // first and last occurrence of the key among the candidates
+    if (threadIdx.x == 0) {
+      int a = r, z = r;
+      while (a > 0 && keys[a - 1] == key) --a;
+      while (z + 1 < n && keys[z + 1] == key) ++z;
+      s_key[j] = key;
+      s_lt[j] = below + a;
+      s_eq[j] = z - a + 1;
+      st->prefix[j] = key;
+    }
+    __syncthreads();
   }
   __syncthreads();
-  if (!last_block) return;
-  __threadfence();
-  // Fixed-order reduction of the per-CTA partials: thread i folds partials i, i+256, ...,
-  // then the block reduces in warp/lane order (deterministic for a given grid).
-  MomentPartial t = {0.0, 0.0, 0ull, 0ull, 0ull, 0ull};
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-    t.s1 += __ldcg(&partials[b].s1);
-    t.lt_first += __ldcg(&partials[b].lt_first);
-    t.eq_first += __ldcg(&partials[b].eq_first);
-    t.lt_last += __ldcg(&partials[b].lt_last);
-    t.eq_last += __ldcg(&partials[b].eq_last);
+  const float v_first = key_float(s_key[0]);
+  const float v_mid = key_float(s_key[1]);
+  const float v_last = key_float(s_key[2]);
+  // Values strictly between the two percentiles: the interior partials plus the candidates
+  // of the boundary ranges (once when the first and last ranges are the same).
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n_partials; i += blockDim.x) acc += __ldcg(&sd.partials[i].s1);
+  const bool same = st->lo[0] == st->lo[2];
+  for (int j = 0; j < 3; j += 2) {
+    if (st->mode[j] != 1 || (j == 2 && same)) continue;
+    const int n = (int)min(st->ncand[j], (unsigned)kSelCands);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float f = key_float(__ldcg(&st->cand[j][i]));
+      if (f > v_first && f < v_last) acc += (double)f;
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    t.s1 += __shfl_down_sync(0xffffffffu, t.s1, o);
-    t.lt_first += __shfl_down_sync(0xffffffffu, t.lt_first, o);
-    t.eq_first += __shfl_down_sync(0xffffffffu, t.eq_first, o);
-    t.lt_last += __shfl_down_sync(0xffffffffu, t.lt_last, o);
-    t.eq_last += __shfl_down_sync(0xffffffffu, t.eq_last, o);
-  }
-  __syncthreads();
-  if (lane == 0) red[warp] = t;
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x != 0) return;
-  t = red[0];
-  for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-    t.s1 += red[w].s1;
-    t.lt_first += red[w].lt_first;
-    t.eq_first += red[w].eq_first;
-    t.lt_last += red[w].lt_last;
-    t.eq_last += red[w].eq_last;
-  }
-  st->ticket = 0;
+  double inner = 0.0;
+  for (int w = 0; w < kSelThreads / 32; ++w) inner += red[w];
+  const int first = sd.first, last = sd.last;
   const long long n = (long long)last - first + 1;
   double s1;
+  long long n_lo, n_hi;
   if (v_first == v_last) {
     s1 = (double)n * v_first;
+    n_lo = n;
+    n_hi = 0;
   } else {
     // Sorted positions holding v_first are [lt_first, lt_first + eq_first - 1], those
     // holding v_last are [lt_last, lt_last + eq_last - 1]; count the ones in [first, last].
-    const long long lo_end = min((long long)t.lt_first + (long long)t.eq_first - 1, (long long)last);
-    const long long n_lo = lo_end - first + 1;
-    const long long n_hi = (long long)last - max((long long)t.lt_last, (long long)first) + 1;
-    s1 = t.s1 + (double)n_lo * v_first + (double)n_hi * v_last;
+    const long long lo_end = min(s_lt[0] + s_eq[0] - 1, (long long)last);
+    n_lo = lo_end - first + 1;
+    n_hi = (long long)last - max(s_lt[2], (long long)first) + 1;
+    s1 = inner + (double)n_lo * v_first + (double)n_hi * v_last;
   }
   const float sum_f = (float)s1;
   const float m = sum_f / (float)n;  // dedoppler.cu:335-336: float sum / count
@@ -266,14 +423,10 @@ __global__ void moments_kernel(const __grid_constant__ SearchBatch b) {
   hdr->mean = m;
   st->mean = m;
   st->n = n;
-  if (v_first == v_last) {
-    st->n_lo = n;
-    st->n_hi = 0;
-  } else {
-    const long long lo_end = min((long long)t.lt_first + (long long)t.eq_first - 1, (long long)last);
-    st->n_lo = lo_end - first + 1;
-    st->n_hi = (long long)last - max((long long)t.lt_last, (long long)first) + 1;
-  }
+  st->n_lo = n_lo;
+  st->n_hi = n_hi;
+  // reset for the next search in this slot
+  for (int j = 0; j < 3; ++j) st->ncand[j] = 0;
 }
 
 
@@ -459,14 +612,19 @@ cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t s
   if (sblocks > 2 * num_sms) sblocks = 2 * num_sms;
   if (sblocks > (maxN + 255) / 256) sblocks = (maxN + 255) / 256;
   dim3 sgrid(sblocks, b.count);
-  // The select passes are latency-bound (a load, three warp votes and shared atomics per
-  // value): many more CTAs than the moment kernels, which need one partial per CTA.
-  int selblocks = (kSelectCtasPerSm * num_sms + b.count - 1) / b.count;
-  if (selblocks > (maxN + 255) / 256) selblocks = (maxN + 255) / 256;
-  if (selblocks < 1) selblocks = 1;
-  dim3 selgrid(selblocks, b.count);
-  for (int shift = 24; shift >= 0; shift -= 8) select_pass<<<selgrid, 256, 0, stream>>>(b, shift);
-  moments_kernel<<<sgrid, 256, 0, stream>>>(b);
+  // Order statistics: the key range, up to three histogram passes (the second and third exit
+  // at once unless a target's bin still holds more than kSelCands values), the compaction
+  // with the interior sum of the mean, and one CTA per search for the exact pick.
+  range_kernel<<<sgrid, 256, 0, stream>>>(b);
+  const int hist_smem = 3 * kSelBins * (int)sizeof(unsigned);
+  cudaError_t e = cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+  if (e != cudaSuccess) return e;
+  int hblocks = (2 * num_sms + b.count - 1) / b.count;
+  if (hblocks > (maxN + 4 * kSelThreads - 1) / (4 * kSelThreads)) hblocks = (maxN + 4 * kSelThreads - 1) / (4 * kSelThreads);
+  if (hblocks < 1) hblocks = 1;
+  for (int pass = 0; pass < 3; ++pass) hist_kernel<<<dim3(hblocks, b.count), kSelThreads, hist_smem, stream>>>(b, pass);
+  compact_kernel<<<sgrid, 256, 0, stream>>>(b);
+  select_finish_kernel<<<dim3(1, b.count), kSelThreads, 0, stream>>>(b, sblocks);
   // The variance emulation walks each chunk in 256-term tiles, one block scan per tile: short
   // chunks (16384 channels) keep that serial walk short.
   int vchunks = std::max(sblocks, (maxN + 16383) / 16384);
