@@ -243,6 +243,35 @@ def test_batch_equals_single_searches(torch_cuda):
     assert sum(len(x) for x in batch) > 70
 
 
+@pytest.mark.parametrize("kind", ["integer", "half_zero"])
+def test_order_statistics_with_heavy_ties(torch_cuda, port_oracle, kind):
+    """Column sums with many equal values: the median and percentile bins hold far more than
+    the 4096 values the exact pick collects, so the histogram passes narrow them to single
+    keys.  Median and mean must equal the oracle's.  The deviation is held to 2e-3: the
+    reference adds the squared deviations in float in the order std::nth_element leaves the
+    array, and with this many exact ties that order decides which terms fall under half an
+    ulp of the running sum (the emulation follows channel order; 4e-4 apart here)."""
+    N = 1 << 18
+    rng = np.random.default_rng(77)
+    x = rng.integers(0, 3, size=(16, N)).astype(np.float32)
+    if kind == "half_zero":
+        x[:, rng.random(N) < 0.6] = 0.0
+    for c, v in ((1000, 40.0), (90000, 30.0), (200000, 25.0)):  # a few drifting tones
+        for t in range(16):
+            x[t, c + t // 4] += v
+    want, wstats = port_oracle.search(x, 2.7939677e-6, 18.253611, 2.0, 0.0, 10.0)
+    got, gstats, _, _ = run_gpu(torch_cuda, x, 2.7939677e-6, 18.253611, 2.0, 0.0, 10.0, T=16)
+    assert gstats.median == np.float32(wstats["median"])
+    assert gstats.mean == np.float32(wstats["mean"])
+    assert abs(gstats.std_dev - wstats["std_dev"]) <= 2e-3 * abs(wstats["std_dev"])
+    # identical hits (no noise path comes near the threshold); SNR follows the deviation
+    assert [(h["index"], h["drift_steps"], np.float32(h["power"])) for h in got] == \
+        [(h["index"], h["drift_steps"], np.float32(h["power"])) for h in want]
+    for a, b in zip(got, want):
+        assert abs(a["snr"] - b["snr"]) <= 2e-3 * abs(b["snr"]), (kind, a, b)
+    assert len(got) >= 3
+
+
 def test_min_drift_filter(torch_cuda, port_oracle):
     """Hits whose |drift rate| is below min_drift are dropped (dedoppler.cu:391)."""
     from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
