@@ -270,19 +270,21 @@ __global__ void __launch_bounds__(256) compact_kernel(const __grid_constant__ Se
     mode[j] = st->mode[j];
   }
   // The ranges of two targets are equal or disjoint (they refine the same bins).  Interior:
-  // keys above the first target's range and below the last's.
+  // keys above the first target's range and below the last's.  After the first histogram a
+  // range is at most 2^20 keys wide, so each test is one 32-bit unsigned compare of k - lo.
   const bool disjoint = lo[0] != lo[2];
-  const unsigned long long in_lo = (unsigned long long)lo[0] + width[0];
-  const uint32_t in_hi = lo[2];
+  const uint32_t in_lo = lo[0] + (uint32_t)width[0];
+  const uint32_t in_len = disjoint ? lo[2] - in_lo : 0u;
+  uint32_t w[3];
+  for (int j = 0; j < 3; ++j) w[j] = mode[j] == 1 ? (uint32_t)width[j] : 0u;  // 0: collects nothing
   const int lane = threadIdx.x & 31;
   double acc = 0.0;
-  for_each_colsum(sd.colsum, sd.N, [&](float f, bool in) {
-    const uint32_t k = sel_key(f);
-    if (in && disjoint && (unsigned long long)k >= in_lo && k < in_hi) acc += (double)f;
+  // Appends the values of lane-local mask bits to the lists: rare (a few thousand values per
+  // search), so it runs only when some lane of the warp holds one.
+  auto collect = [&](uint32_t k, bool t0, bool t1, bool t2) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      if (mode[j] != 1) continue;
-      const bool take = in && k >= lo[j] && (unsigned long long)(k - lo[j]) < width[j];
+      const bool take = j == 0 ? t0 : (j == 1 ? t1 : t2);
       const unsigned m = __ballot_sync(0xffffffffu, take);
       if (m == 0) continue;
       const int leader = __ffs(m) - 1;
@@ -294,7 +296,40 @@ __global__ void __launch_bounds__(256) compact_kernel(const __grid_constant__ Se
         if (at < (unsigned)kSelCands) st->cand[j][at] = k;
       }
     }
-  });
+  };
+  const float* __restrict__ x = sd.colsum;
+  const int N = sd.N;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+  const int n4 = vec ? N / 4 : 0;
+  const int r4 = (n4 + stride - 1) / stride * stride;
+  for (int i = tid; i < r4; i += stride) {
+    const bool in = i < n4;
+    const float4 v = in ? __ldg(reinterpret_cast<const float4*>(x) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float f[4] = {v.x, v.y, v.z, v.w};
+    uint32_t k[4];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      k[q] = sel_key(f[q]);
+      if (in && k[q] - in_lo < in_len) acc += (double)f[q];
+      any |= in && ((k[q] - lo[0] < w[0]) | (k[q] - lo[1] < w[1]) | (k[q] - lo[2] < w[2]));
+    }
+    if (__ballot_sync(0xffffffffu, any) == 0u) continue;  // the common case: no candidate in the warp
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      collect(k[q], in && k[q] - lo[0] < w[0], in && k[q] - lo[1] < w[1], in && k[q] - lo[2] < w[2]);
+  }
+  const int rest = N - 4 * n4;
+  const int rr = (rest + stride - 1) / stride * stride;
+  for (int i = tid; i < rr; i += stride) {
+    const bool in = i < rest;
+    const float f = in ? x[4 * n4 + i] : 0.0f;
+    const uint32_t k = sel_key(f);
+    if (in && k - in_lo < in_len) acc += (double)f;
+    collect(k, in && k - lo[0] < w[0], in && k - lo[1] < w[1], in && k - lo[2] < w[2]);
+  }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if (lane == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
@@ -444,13 +479,16 @@ __device__ __forceinline__ float var_term(float f, float m) {
 
 __device__ __forceinline__ bool var_inside(float f, float lo, float hi) { return f > lo && f < hi; }
 
+// Channels per variance chunk: a multiple of 8, so every chunk starts 32-byte aligned.
+__device__ __forceinline__ int var_chunk_len(int N, int chunks) { return ((N + chunks - 1) / chunks + 7) & ~7; }
+
 // Per-chunk exact sums of the terms of the channels strictly between the percentiles.
 __global__ void var_chunk_kernel(const __grid_constant__ SearchBatch b) {
   const SearchDesc& sd = b.s[blockIdx.y];
   const float* __restrict__ x = sd.colsum;
   const int N = sd.N;
   const SelectState* st = sd.sel;
-  const int chunk = (N + gridDim.x - 1) / gridDim.x;
+  const int chunk = var_chunk_len(N, gridDim.x);
   double* chunk_sum = sd.var;
   __shared__ double red[32];
   const float lo = key_float(st->prefix[0]), hi = key_float(st->prefix[2]);
@@ -506,7 +544,7 @@ __global__ void var_emulate_kernel(const __grid_constant__ SearchBatch b) {
   const float* __restrict__ x = sd.colsum;
   const int N = sd.N;
   SelectState* st = sd.sel;
-  const int chunk = (N + gridDim.x - 1) / gridDim.x;
+  const int chunk = var_chunk_len(N, gridDim.x);
   const double* chunk_sum = sd.var;
   double* chunk_part = sd.var + kVarChunks;
   const double snr_threshold = sd.snr_threshold;
@@ -529,17 +567,38 @@ __global__ void var_emulate_kernel(const __grid_constant__ SearchBatch b) {
   const long long b0 = (long long)blockIdx.x * chunk;
   const long long b1 = min((long long)N, b0 + chunk);
   double contrib = 0.0;
-  for (long long t0 = b0; t0 < b1; t0 += blockDim.x) {
-    const long long i = t0 + threadIdx.x;
-    double term = 0.0;
-    if (i < b1) {
-      const float f = x[i];
-      if (var_inside(f, lo, hi)) term = (double)var_term(f, m);
+  // Tiles of 8 consecutive channels per thread: one block scan per 8 * blockDim.x channels;
+  // each thread then walks its 8 in channel order.  The ulp of a float is a power of two,
+  // so term / ulp is the exact product with its reciprocal.
+  constexpr int K = 8;
+  const bool vec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  for (long long t0 = b0; t0 < b1; t0 += (long long)blockDim.x * K) {
+    const long long i0 = t0 + (long long)threadIdx.x * K;
+    float v[K];
+    if (vec && i0 + K <= b1) {
+      const float4 p = __ldg(reinterpret_cast<const float4*>(x + i0));
+      const float4 q = __ldg(reinterpret_cast<const float4*>(x + i0) + 1);
+      v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
+      v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[k] = (i0 + k < b1) ? x[i0 + k] : lo;  // lo: not inside
     }
-    const double pre = block_exclusive_scan(term, warp_tot, &tile_total);
-    if (term != 0.0) {
-      const double u = float_ulp_above(base + pre);
-      contrib += rint(term / u) * u;
+    double term[K];
+    double tsum = 0.0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      term[k] = var_inside(v[k], lo, hi) ? (double)var_term(v[k], m) : 0.0;
+      tsum += term[k];
+    }
+    double a = base + block_exclusive_scan(tsum, warp_tot, &tile_total);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (term[k] != 0.0) {
+        const double u = float_ulp_above(a);
+        contrib += rint(term[k] * __drcp_rn(u)) * u;
+      }
+      a += term[k];
     }
     base += tile_total;
   }
