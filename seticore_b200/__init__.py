@@ -11,6 +11,7 @@ from .dedoppler import (  # noqa: F401
     Dedopplerer,
     FilterbankBuffer,
     FilterbankMetadata,
+    HitList,
     driftStepsLessThan,
     makeNoisyBuffer,
     roundUpToPowerOfTwo,

@@ -12,6 +12,7 @@ path: a search on a tensor that is not on a CUDA device raises.
 """
 import ctypes
 import math
+from collections.abc import Sequence
 from dataclasses import dataclass, field
 from typing import List, Optional
 
@@ -188,6 +189,38 @@ def _device_input(input, num_rows: int, num_channels: int):
     return t
 
 
+class HitList(Sequence):
+    """The hit records (ScDdHit) of one search from the raw calls.  The records are held in
+    one private copy; a record object is made only when the list is indexed or iterated, so
+    a call that returns thousands of hits does not build thousands of Python objects."""
+
+    __slots__ = ("_records",)
+
+    def __init__(self, records):
+        self._records = records
+
+    def __len__(self):
+        return len(self._records)
+
+    def __getitem__(self, i):
+        return self._records[i]
+
+    def __iter__(self):
+        return iter(self._records)
+
+    def __eq__(self, other):
+        if isinstance(other, (list, tuple, HitList)):
+            return len(self) == len(other) and all(a is b or _same_hit(a, b) for a, b in zip(self, other))
+        return NotImplemented
+
+    def __repr__(self):
+        return f"HitList({len(self)} hits)"
+
+
+def _same_hit(a, b) -> bool:
+    return all(getattr(a, f) == getattr(b, f) for f, _ in _capi.ScDdHit._fields_)
+
+
 def _stream_handle(stream):
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
@@ -282,18 +315,29 @@ class Dedopplerer:
         return buf
 
     @staticmethod
-    def _copy_hits(buf, start: int, count: int) -> list:
+    def _copy_hits(buf, start: int, count: int) -> "HitList":
         """Records [start, start + count) of the reusable buffer, copied out (the buffer is
         overwritten by the next call)."""
-        out = (_capi.ScDdHit * count)()
-        if count:
-            size = ctypes.sizeof(_capi.ScDdHit)
-            ctypes.memmove(out, ctypes.addressof(buf) + start * size, count * size)
-        return list(out)
+        return Dedopplerer._split_hits(buf, [count], start)[0]
+
+    @staticmethod
+    def _split_hits(buf, counts, start: int = 0) -> list:
+        """One HitList per count over consecutive records of the reusable buffer from `start`:
+        a single copy of all of them, then views into it."""
+        size = ctypes.sizeof(_capi.ScDdHit)
+        total = sum(counts)
+        block = (_capi.ScDdHit * max(total, 1))()
+        if total:
+            ctypes.memmove(block, ctypes.addressof(buf) + start * size, total * size)
+        out, k = [], 0
+        for c in counts:
+            out.append(HitList((_capi.ScDdHit * c).from_buffer(block, k * size)))
+            k += c
+        return out
 
     def search_raw(self, input, beam: int, coarse_channel: int, max_drift: float,
                    min_drift: float, snr_threshold: float, stream=None, capacity: int = 4096):
-        """Runs the search and returns the C ABI hit records (list of ScDdHit)."""
+        """Runs the search and returns the C ABI hit records (a HitList of ScDdHit)."""
         t = _device_input(input, self.rounded_num_timesteps, self.num_channels)
         cap = capacity
         while True:
@@ -311,7 +355,7 @@ class Dedopplerer:
     def search_batch_raw(self, inputs, beams, coarse_channels, max_drift: float, min_drift: float,
                          snr_threshold: float, stream=None, capacity: int = 1 << 16):
         """Many searches of this engine's shape in one call (sc_dd_search_batch).  Returns one
-        list of ScDdHit per input."""
+        HitList of ScDdHit per input."""
         ts = [_device_input(x, self.rounded_num_timesteps, self.num_channels) for x in inputs]
         n = len(ts)
         if n == 0:
@@ -330,11 +374,7 @@ class Dedopplerer:
                 cap = sum(counts)
                 continue
             check(rc)
-            out, k = [], 0
-            for cnt in counts:
-                out.append(self._copy_hits(buf, k, cnt))
-                k += cnt
-            return out
+            return self._split_hits(buf, list(counts))
 
     def search_batch(self, inputs, metadata: Optional[FilterbankMetadata], beams, coarse_channels,
                      max_drift: float, min_drift: float, snr_threshold: float, stream=None) -> list:

@@ -72,7 +72,7 @@ class SearchPool:
         return int(lib().sc_dd_request_scratch_bytes(ctypes.byref(r)))
 
     def search_raw(self, requests: List[SearchRequest], stream=None, capacity: int = 1 << 16):
-        """One list of ScDdHit per request."""
+        """One HitList of ScDdHit per request."""
         n = len(requests)
         if n == 0:
             return []
@@ -88,11 +88,7 @@ class SearchPool:
                 cap = sum(counts)
                 continue
             check(rc, pool=True)
-            out, k = [], 0
-            for c in counts:
-                out.append(Dedopplerer._copy_hits(buf, k, c))
-                k += c
-            return out
+            return Dedopplerer._split_hits(buf, list(counts))
 
     def stats(self) -> _capi.ScDdPoolStats:
         s = _capi.ScDdPoolStats()
