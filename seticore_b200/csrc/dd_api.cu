@@ -355,6 +355,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
       return cuda_fail(e, "result copy");
     for (int k = 0; k < n; ++k) {
       const scb::SearchHeader h = dd->host_hdrs()[k];
+      if (h.error) return fail(SC_DD_EINTERNAL, "a tree kernel gave up waiting for its staged rows");
       const int ncand = std::min(h.num_candidates, dd->cand_cap);
       std::vector<scb::Candidate> cands(ncand);
       const scb::Candidate* hc = dd->host_cands() + (size_t)kHostCands * k;

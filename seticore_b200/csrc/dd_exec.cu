@@ -8,6 +8,7 @@
 //   sums -> levels for more than 32 rows, one search at a time -> statistics ->
 //   [flag + FP32 recompute of the flagged channels] -> hits
 #include <algorithm>
+#include <cstddef>
 
 #include "dd_common.cuh"
 #include "dd_internal.h"
@@ -87,6 +88,11 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
 bool tree_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 32 && e.dmin <= 0 && e.dmax >= 0; }
 bool fused_colsum(const ExecSearch& e) { return tree_colsum(e) || e.elem != kElemF32; }
 
+// The search's header word that a kernel sets when it gives up a wait.
+int* header_status(const ExecSearch& e) {
+  return reinterpret_cast<int*>(reinterpret_cast<char*>(e.hdr) + offsetof(SearchHeader, error));
+}
+
 TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride, float* top) {
   TreeGroup g{};
   g.rows = rows;
@@ -102,6 +108,7 @@ TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride
   g.off_step = 0;
   g.elig_T1 = e.Tr - 1;
   g.top = top;
+  g.status = header_status(e);
   return g;
 }
 
@@ -193,13 +200,14 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       if (ss[k].Tr <= 32) continue;
       if (ss[k].elem != kElemF32) {
         if ((e = levels_search(ss[k].norm16, ss[k].N, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
-                               ss[k].top16, num_sms, stream, LevelPlan{}, ss[k].elem)) != cudaSuccess)
+                               ss[k].top16, num_sms, stream, LevelPlan{}, ss[k].elem, header_status(ss[k]))) !=
+            cudaSuccess)
           return e;
         continue;
       }
       const LevelPlan plan = hooks.level_plan ? hooks.level_plan(hooks.ctx, ss[k], lvl_a, lvl_b, stream) : ss[k].level_plan;
       if ((e = levels_search(ss[k].input, ss[k].row_stride, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
-                             ss[k].top, num_sms, stream, plan)) != cudaSuccess)
+                             ss[k].top, num_sms, stream, plan, kElemF32, header_status(ss[k]))) != cudaSuccess)
         return e;
     }
     if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);

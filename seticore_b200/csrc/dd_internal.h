@@ -81,7 +81,7 @@ struct Candidate {
 // Device-side result block of one search; the candidates follow it in memory.
 struct SearchHeader {
   int num_candidates;
-  int error;
+  int error;  // nonzero: a kernel of the search gave up a wait (the results are invalid)
   int pad0, pad1;
   float median, std_dev, mean, threshold;
 };
@@ -144,6 +144,8 @@ struct TreeGroup {
   int n_chunks;
   int n_tiles;
   int item_begin;  // first work item of this group in the launch
+  // Optional: set to 1 if a staging wait of the tree gave up (its results are then invalid).
+  int* status;
 };
 
 struct TreeBatch {
@@ -247,7 +249,8 @@ struct LevelPlan {
 // only the default plan reads: its first level converts on load).
 cudaError_t levels_search(const void* input, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
-                          cudaStream_t stream, const LevelPlan& plan = LevelPlan{}, int elem = kElemF32);
+                          cudaStream_t stream, const LevelPlan& plan = LevelPlan{}, int elem = kElemF32,
+                          int* status = nullptr);
 
 // A fully planned search for exec_queue: the request, its drift plan and its scratch.
 struct ExecSearch {

@@ -174,7 +174,7 @@ TreeGroup final_group(const float* src, long long Np, int N, int final_rows, int
 // group q reads rows 16q .. 16q + 15 (one trapezoid for the nj drift blocks) and writes
 // plane r*(Tr/16) + q of drift block j to out + j*job_stride.
 cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long long Np, int db0, int nj,
-                   float* out, long long job_stride, int num_sms, cudaStream_t stream) {
+                   float* out, long long job_stride, int num_sms, cudaStream_t stream, int* status) {
   const int nb = Tr / 16;
   TreeBatch eb;
   eb.count = nb;
@@ -192,6 +192,7 @@ cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long
     g.emit_out = out + (long long)q * Np;
     g.emit_job_stride = job_stride;
     g.emit_plane_stride = (long long)nb * Np;
+    g.status = status;
   }
   return tree_emit_batch(eb, num_sms, stream);
 }
@@ -200,7 +201,7 @@ cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long
 
 cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
-                          cudaStream_t stream, const LevelPlan& plan, int elem) {
+                          cudaStream_t stream, const LevelPlan& plan, int elem, int* status) {
   int sizes[12];
   int nlev = 0;
   int final_rows = 16;
@@ -244,7 +245,7 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
     for (int db = dmin; db <= dmax; db += (int)J) {
       const int nj = (int)std::min<long long>(J, dmax - db + 1);
       if (sizes[0] == kStreamEmit16) {
-        if ((err = emit16(input, row_stride, Tr, N, Np, db, nj, scratch_a, per_db, num_sms, stream)) != cudaSuccess)
+        if ((err = emit16(input, row_stride, Tr, N, Np, db, nj, scratch_a, per_db, num_sms, stream, status)) != cudaSuccess)
           return err;
       } else {
         dim3 grid((N + 511) / 512, (unsigned)(nj * nb));
@@ -260,8 +261,10 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
       TreeBatch tb;
       tb.count = nj;
       tb.n_items = 0;
-      for (int j = 0; j < nj; ++j)
+      for (int j = 0; j < nj; ++j) {
         tb.g[j] = final_group(scratch_a + j * per_db, Np, N, final_rows, 16, 16, db + j, Tr, top);
+        tb.g[j].status = status;
+      }
       if ((err = tree_max_batch(tb, final_rows, num_sms, stream)) != cudaSuccess) return err;
     }
     return cudaGetLastError();
@@ -278,7 +281,7 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
       const int D0 = (int)(dscale * db);
       if (M == kStreamEmit16) {
         M = 16;
-        if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, per_db, num_sms, stream)) != cudaSuccess) return err;
+        if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, per_db, num_sms, stream, status)) != cudaSuccess) return err;
       } else if (M == 16) {
         dim3 grid((N + 511) / 512, (unsigned)(P * (Tp / M)));
         if (l == 0 && elem == kElemBF16) {
@@ -309,6 +312,7 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
     tb.count = 1;
     tb.n_items = 0;
     tb.g[0] = final_group(src, Np, N, final_rows, P, dscale, db, Tr, top);
+    tb.g[0].status = status;
     if ((err = tree_max_batch(tb, final_rows, num_sms, stream)) != cudaSuccess) return err;
   }
   return cudaGetLastError();

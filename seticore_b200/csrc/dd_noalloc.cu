@@ -177,6 +177,7 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   tp.off_step = 0;
   tp.elig_T1 = Tr - 1;
   tp.top = top;
+  tp.status = &hdr->error;  // an address inside the device array, not a host read
   if ((e = scb::tree_max_batch(tb, Tr, num_sms, stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: tree kernel");
   if ((e = scb::search_hits_batch(batch, num_sms, stream)) != cudaSuccess)
@@ -187,6 +188,7 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   if ((e = cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(stream)) != cudaSuccess)
     return cuda_fail(e, "sc_dd_search_static: result copy");
+  if (h.error) return fail(SC_DD_EINTERNAL, "sc_dd_search_static: a tree kernel gave up a wait");
   const int ncand = std::min(h.num_candidates, kStaticMaxCands);
   scb::Candidate chunk[kHostChunk];
   int n = 0;

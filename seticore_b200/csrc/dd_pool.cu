@@ -19,6 +19,7 @@
 // CUDA graphs: a sub-batch seen before (same requests, same arena layout) is replayed
 // from a captured graph that also holds the copies of the results to pinned host memory.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -209,8 +210,9 @@ scb::LevelPlan pool_level_plan(void* ctx, const scb::ExecSearch& s, float* la, f
   float best_ms = 1e30f;
   for (const scb::LevelPlan& pl : level_candidates(s.Tr)) {
     cudaEventRecord(p->t0, st);
-    if (scb::levels_search(s.input, s.row_stride, s.Tr, s.N, s.dmin, s.dmax, la, lb, s.top, p->num_sms, st, pl) !=
-        cudaSuccess)
+    int* status = reinterpret_cast<int*>(reinterpret_cast<char*>(s.hdr) + offsetof(scb::SearchHeader, error));
+    if (scb::levels_search(s.input, s.row_stride, s.Tr, s.N, s.dmin, s.dmax, la, lb, s.top, p->num_sms, st, pl,
+                           scb::kElemF32, status) != cudaSuccess)
       continue;
     cudaEventRecord(p->t1, st);
     cudaEventSynchronize(p->t1);
@@ -495,6 +497,7 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
     for (size_t k = 0; k < sub.size(); ++k, h += sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands) {
       const Planned& pl = sub[k];
       const scb::SearchHeader hd = *reinterpret_cast<const scb::SearchHeader*>(h);
+      if (hd.error) return pfail(SC_DD_EINTERNAL, "a tree kernel gave up waiting for its staged rows");
       const int ncand = std::min(hd.num_candidates, pl.es.cand_cap);
       const int head = std::min(kHostCands, pl.es.cand_cap);
       std::vector<scb::Candidate> cands(ncand);
