@@ -38,9 +38,13 @@ MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.34 MB +
-# 15.31 MB); a launch covering k coarse channels moves k times this.
-TREE_DRAM_BYTES = 78148288
+# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.93 MB +
+# 26.87 MB); a launch covering k coarse channels moves k times this.
+TREE_DRAM_BYTES = 78198528
+# Kernels of one FP32 batch of up to 64 searches of at most 32 rows: clear, tree, range,
+# three histogram passes, compaction, order-statistic finish, two variance kernels, window,
+# drift recovery.
+LAUNCHES_PER_BATCH = 12
 
 
 def dist_setup():
@@ -553,7 +557,7 @@ def main():
             "precision_forms": precision,
             # per batch of up to 64 coarse channels: clear, tree (with the column sums), four
             # select passes, moments, two variance kernels, window and resolve
-            "gpu_launches": len(tree_ms) * 11 * ((n_coarse + 63) // 64),
+            "gpu_launches": len(tree_ms) * LAUNCHES_PER_BATCH * ((n_coarse + 63) // 64),
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline("reference", steps=1)
