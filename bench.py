@@ -310,7 +310,7 @@ def run_serve(args, world, rank, local):
 
 def run_beams(args, world, rank, local):
     """Beamformed-style case: 64 beams x 256 timesteps x 131072 channels (foff 3.81 Hz,
-    tsamp 0.268 s, max_drift 10 Hz/s), one batched call; more than 16 rows, so the
+    tsamp 0.268 s, max_drift 10 Hz/s), one batched call; more than 32 rows, so the
     level path runs."""
     import torch
     from seticore_b200 import Dedopplerer

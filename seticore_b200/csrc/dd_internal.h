@@ -170,7 +170,7 @@ cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream
 
 // The same staged tree for 16 rows, writing every root value (all 16 in-block offsets of
 // every channel) to the groups' emit planes instead of folding maxima: the first level of
-// a tree of more than 16 rows.  Values of paths that leave [0, N) are sums with zeros.
+// a tree of more than 32 rows.  Values of paths that leave [0, N) are sums with zeros.
 // Every tile is stored whole, so plane rows must hold level_row_length(N) floats.
 cudaError_t tree_emit_batch(TreeBatch& b, int num_sms, cudaStream_t stream, int smem_budget_kb = 0);
 
@@ -218,7 +218,7 @@ cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream
 cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
 
 // Column sums of each search (searches whose tree computes them skip this); also resets
-// each search's radix-select state.
+// each search's order-statistic state.
 cudaError_t column_sums_batch(const SearchBatch& b, cudaStream_t stream);
 // Order statistics, mean, standard deviation and threshold of each search, from its column
 // sums and a reset select state (column_sums_batch or exec_queue's clear launch).
@@ -231,7 +231,7 @@ cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t st
 cudaError_t path_values(const float* input, long long row_stride, int Tr, int N, const int* index,
                         const int* drift_steps, float* out, int n, cudaStream_t stream);
 
-// How a tree of more than 16 rows is split: levels of m[0..n) rows each -- 2 or 4
+// How a tree of more than 32 rows is split: levels of m[0..n) rows each -- 2 or 4
 // (emit_kernel), 8 or 16 (direct_kernel, one thread per channel) or, first only,
 // kStreamEmit16 (the emitting form of the fused tree) -- then a fused max level of
 // final_rows (2, 4, 8 or 16) rows.  n == 0: the default split.
@@ -242,7 +242,7 @@ struct LevelPlan {
   int final_rows;
 };
 
-// Multi-level tree for Tr > 16 (one search): level kernels write the partial planes of
+// Multi-level tree for Tr > 32 (one search): level kernels write the partial planes of
 // every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).
 // scratch_a / scratch_b: level_buffer_floats(Tr, N) floats each, in one allocation.
 // `input` holds elements of type `elem` (float, or the precision form's 16-bit copy, which
@@ -286,7 +286,7 @@ struct ExecHooks {
   void* ctx = nullptr;
   TreeLaunch (*tree_launch)(void* ctx, const TreeBatch& tb, int R, int elem) = [](void*, const TreeBatch&, int,
                                                                                    int) { return TreeLaunch{}; };
-  // The level split of a search with more than 16 rows (may time alternatives first).
+  // The level split of a search with more than 32 rows (may time alternatives first).
   LevelPlan (*level_plan)(void* ctx, const ExecSearch& s, float* lvl_a, float* lvl_b, cudaStream_t st) = nullptr;
   void (*before_tree)(void* ctx, cudaStream_t s) = nullptr;
   void (*after_tree)(void* ctx, cudaStream_t s) = nullptr;
@@ -294,7 +294,7 @@ struct ExecHooks {
 
 // Queues every kernel of n searches (any mix) on `stream`; no synchronisation.
 // lvl_a / lvl_b: level buffers of level_buffer_floats(Tr, N) floats for every search with
-// Tr > 16, in one allocation.
+// Tr > 32, in one allocation.
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
                        const ExecHooks& hooks);
 

@@ -12,7 +12,7 @@
 // timed with each candidate launch shape -- tile width (1056 or 352 channels) and
 // shared-memory budget (which sets how many drift blocks share a staged trapezoid and how
 // many CTAs share an SM) -- and the fastest is kept; likewise, each
-// class of more than 16 rows (rows, buckets of channels and drift blocks) times the
+// class of more than 32 rows (rows, buckets of channels and drift blocks) times the
 // candidate level splits (stage-fusion depth).  Timing reruns are harmless: the tree
 // kernel only raises per-channel maxima, so repeating it is idempotent.
 //

@@ -22,7 +22,7 @@ offset half small enough for the instruction cache.  Each channel's outputs are 
 a running maximum (starting at 0, so NaN and negative sums never count) that fold_max()
 merges into the CTA's per-channel maxima in shared memory.  The emitting form
 (taylor_strip_emit) hands every root value to a sink instead: the first level of a tree of
-more than 16 rows, whose output planes the next level reads.
+more than 32 rows, whose output planes the next level reads.
 """
 import os
 import sys
