@@ -136,6 +136,22 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
                 body.append((s, R, f"    sink.put({i}, base + {s}, {e});"))
             continue
         body.append((s, R, f"    float m{s} = 0.0f;"))
+        # Offsets 2q and 2q + 1 share their left operand: their larger sum is
+        # left + max(right at +q, right at +q + 1), exactly (rounding is monotonic, and a NaN
+        # sum never counts on either side), so the pair costs one add and one max.
+        outs = []
+        his = {o for (_, _, o) in roots}
+        for (_, _, o) in roots:
+            q = o // 2
+            if o % 2 == 0 and o + 1 in his:
+                left = body_name(R // 2, 0, q, s)
+                r0, r1 = body_name(R // 2, 1, q, s + q), body_name(R // 2, 1, q, s + q + 1)
+                outs.append(f"{left} + fmaxf({r0}, {r1})")
+            elif o % 2 == 1 and o - 1 in his:
+                continue
+            else:
+                sh = (o + 1) // 2
+                outs.append(f"{body_name(R // 2, 0, q, s)} + {body_name(R // 2, 1, q, s + sh)}")
         for i, e in enumerate(outs):
             body.append((s, R, f"    const float o{s}_{i} = {e};"))
         acc = f"m{s}"
