@@ -496,7 +496,17 @@ __global__ void var_chunk_kernel(const __grid_constant__ SearchBatch b) {
   const long long b0 = (long long)blockIdx.x * chunk;
   const long long b1 = min((long long)N, b0 + chunk);
   double acc = 0.0;
-  for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+  // 16-byte loads over the chunk (chunks start 32-byte aligned), then the ragged end.
+  const bool vec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  const long long n4 = vec ? (b1 - b0) / 4 : 0;
+  for (long long i = threadIdx.x; i < n4; i += blockDim.x) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(x + b0) + i);
+    if (var_inside(v.x, lo, hi)) acc += (double)var_term(v.x, m);
+    if (var_inside(v.y, lo, hi)) acc += (double)var_term(v.y, m);
+    if (var_inside(v.z, lo, hi)) acc += (double)var_term(v.z, m);
+    if (var_inside(v.w, lo, hi)) acc += (double)var_term(v.w, m);
+  }
+  for (long long i = b0 + 4 * n4 + threadIdx.x; i < b1; i += blockDim.x) {
     const float f = x[i];
     if (var_inside(f, lo, hi)) acc += (double)var_term(f, m);
   }
