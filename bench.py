@@ -38,9 +38,9 @@ MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.93 MB +
-# 26.87 MB); a launch covering k coarse channels moves k times this.
-TREE_DRAM_BYTES = 78198528
+# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.94 MB +
+# 26.43 MB); a launch covering k coarse channels moves k times this.
+TREE_DRAM_BYTES = 78093248
 # Kernels of one FP32 batch of up to 64 searches of at most 32 rows: clear, tree, range,
 # three histogram passes, compaction, order-statistic finish, two variance kernels, window,
 # drift recovery.
