@@ -28,7 +28,8 @@ enum {
   SC_DD_ECUDA = 2,     /* a CUDA runtime call failed */
   SC_DD_ENOMEM = 3,    /* device or pinned allocation failed */
   SC_DD_ETRUNC = 4,    /* more hits than the caller's capacity; *num_hits is the total */
-  SC_DD_EINTERNAL = 5, /* a device-side consistency check failed */
+  SC_DD_EINTERNAL = 5, /* a device-side consistency check failed, or a kernel gave up a bounded
+                          wait for its staged rows (the results of that call are invalid) */
   SC_DD_ESHAPE = 6,    /* input shape differs from the engine's (dedoppler.cu:191-192) */
   SC_DD_ELIMIT = 7     /* a size exceeds the stated maximum of sc_dd_search_static */
 };
