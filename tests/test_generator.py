@@ -60,7 +60,7 @@ def _fmaxf(a, b):
     return a if a >= b else b
 
 
-def _run(code, rows, S, emit=False, n_out=0):
+def _run(code, rows, S, emit=False):
     F0 = np.float32(0.0)
     top = [F0] * S
     vals = {}
@@ -141,3 +141,38 @@ def test_root_pairs_and_reload_are_used():
     code = gen.gen_strip_loop(16, 0, 16, 11, 3, reload=8)
     assert code.count("fmaxf(") == 11 * 8  # eight pairs per channel, eleven channels per iteration
     assert "s1_15_0" not in code and "s1_7_0" in code  # leaf 15's window is reread, leaf 7's carried
+
+
+def _run_direct(code, rows, CH):
+    """Runs a generated taylor_direct_M function: ld(t, pos) = rows[t][pos]."""
+    body = []
+    for raw in code.splitlines():
+        s = raw.strip()
+        if not s or s.startswith("template") or s.startswith("__device__") or s == "}":
+            continue
+        s = s.rstrip(";")
+        s = re.sub(r"^const float ", "", s)
+        body.append(s)
+    out, sunk = {}, {}
+
+    def sink(o, *vals):
+        for j, v in enumerate(vals):
+            sunk[(o, j)] = v
+
+    env = {"ld": lambda t, pos: rows[t][pos], "out": out, "sink": sink}
+    exec(compile("\n".join(body), "<generated>", "exec"), env)
+    if CH == 1:
+        return {(o, 0): v for o, v in out.items()}
+    return sunk
+
+
+@pytest.mark.parametrize("M,CH", [(m, 1) for m in gen.DIRECT_SIZES] + list(gen.DIRECT_MULTI))
+def test_direct_level_equals_recursion(M, CH):
+    """The one-level subtrees of the level path: all M offsets at CH consecutive channels."""
+    for seed in range(3):
+        rows = _rows(M, CH + M, 300 + 10 * M + seed)
+        got = _run_direct(gen.gen_direct(M, CH), rows, CH)
+        ref = _reference(rows, M, 0, M, CH)
+        assert set(got) == set(ref)
+        for key, v in ref.items():
+            assert np.float32(got[key]).tobytes() == v.tobytes(), (M, CH, seed, key)
