@@ -239,7 +239,7 @@ def gen_direct(M, CH=1):
 # (R, offset parts, U steps per iteration, iterations[, reload]) compiled into the library; a
 # strip is S = U * ITERS channels (odd, so a warp's 32 strips start in 32 distinct banks);
 # reload: leaves with windows of that many positions or more are read again at each use.
-LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 1, 11, 3, 8),
+LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 1, 11, 3, 12), (16, 1, 11, 3, 8),
                 # 32 rows in two parts of sixteen offsets
                 (32, 2, 11, 3),
                 # short strips (S = 11) for launches whose jobs each stage their own rows

@@ -138,9 +138,9 @@ def test_emit_form_writes_every_root_value(R, nparts, U, IT):
 
 def test_root_pairs_and_reload_are_used():
     """The 16-row long-strip form folds its roots in pairs and reads wide leaves again."""
-    code = gen.gen_strip_loop(16, 0, 16, 11, 3, reload=8)
+    code = gen.gen_strip_loop(16, 0, 16, 11, 3, reload=12)
     assert code.count("fmaxf(") == 11 * 8  # eight pairs per channel, eleven channels per iteration
-    assert "s1_15_0" not in code and "s1_7_0" in code  # leaf 15's window is reread, leaf 7's carried
+    assert "s1_15_0" not in code and "s1_11_0" in code  # leaf 15's window is reread, leaf 11's carried
 
 
 def _run_direct(code, rows, CH):
