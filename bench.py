@@ -38,9 +38,9 @@ MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.94 MB +
-# 26.43 MB); a launch covering k coarse channels moves k times this.
-TREE_DRAM_BYTES = 78093248
+# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 286.21 MB +
+# 29.11 MB); a launch covering k coarse channels moves k times this.
+TREE_DRAM_BYTES = 78829184
 # Kernels of one FP32 batch of up to 64 searches of at most 32 rows: clear, tree, range,
 # three histogram passes, compaction, order-statistic finish, two variance kernels, window,
 # drift recovery.
@@ -542,7 +542,7 @@ def main():
     achieved = alg / (tree_launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (TREE_DRAM_BYTES * per_launch if TREE_DRAM_BYTES else None), "peak_source": peak_src,
-                "kernel": "tree_max_kernel<float,16,1,33> (8 warps, 2 CTAs per SM, leaves reloaded from 8)", "searches_per_launch": per_launch,
+                "kernel": "tree_max_kernel<float,16,1,33> (8 warps, 2 CTAs per SM, leaves reread from 12)", "searches_per_launch": per_launch,
                 "kernel_ms": tree_launch_ms, "algorithmic_bytes_per_launch": alg,
                 "note": "algorithmic bytes assume one tree read per drift block; the fused kernel stages each "
                         "input tile once for all drift blocks, so frac > 1 is expected"}
