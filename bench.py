@@ -13,6 +13,11 @@ copy of every coarse channel is inside the timed region (copies overlap the prev
 channel's search on a second stream).  Multi-GPU runs are independent replicas (weak
 scaling): every rank searches its own node; nothing is exchanged.
 
+A 1-GPU run also adds, as extra keys of the same line, the other workloads with a few timed
+steps each: "beams" (64 x 256 x 131072, the level path), "uneven" (512 searches of mixed
+shapes through the pool) and "serve" (Poisson arrivals of the uneven mix, p50/p99).  Each
+also runs alone with --workload.
+
 --impl reference times the reference's own CPU Taylor path (oracle/_ref/libref_cpu.so:
 the reference's taylorOneStepOneChannel over all channels, all host threads) on a
 bounded sample of the same workload.
@@ -41,6 +46,12 @@ UNIT = "Gsamples/s"
 # dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 286.21 MB +
 # 29.11 MB); a launch covering k coarse channels moves k times this.
 TREE_DRAM_BYTES = 78829184
+# Warp instructions the tree kernel executes per coarse channel of the node (ncu
+# smsp__inst_executed.sum of the same capture: 744.2 M for 4 coarse channels).
+TREE_WARP_INSTR = 744.2e6 / 4
+# Level path of the beams workload, DRAM bytes per beam of 256 x 131072 (2 drift blocks):
+# direct16x4_kernel 268.5 + 223.2 MB and the last level 269.5 + 3.8 MB (ncu, one launch each).
+BEAMS_DRAM_BYTES = 765.0e6
 # Kernels of one FP32 batch of up to 64 searches of at most 32 rows: clear, tree, range,
 # three histogram passes, compaction, order-statistic finish, two variance kernels, window,
 # drift recovery.
@@ -113,16 +124,29 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes_fp32(Tr, n, ndb):
-    """Per search: one stats read, one tree read per drift block, a (sum, drift, offset)
-    write per channel: 4*Tr*N*(ndb+1) + 12*N."""
+def bytes_read_per_drift_block(Tr, n, ndb):
+    """The reference's schedule, per search: one stats read, one tree read per drift block and
+    a (sum, drift, offset) write per channel: 4*Tr*N*(ndb+1) + 12*N.  The fused tree reads its
+    input about once, so this is not a bound for it; it is reported only under this name."""
     return 4 * Tr * n * (ndb + 1) + 12 * n
 
 
-def algorithmic_bytes_16bit(Tr, n, ndb):
-    """Per search of the 16-bit forms: the float32 read and 16-bit write of normalisation,
-    one 16-bit tree read per drift block and the per-channel write: 6*Tr*N + 2*Tr*N*ndb + 12*N."""
-    return 6 * Tr * n + 2 * Tr * n * ndb + 12 * n
+def bytes_fused_fp32(Tr, n):
+    """What the fused FP32 tree must move per search: the input read once and the per-channel
+    top sums and column sums written, 4*Tr*N + 8*N."""
+    return 4 * Tr * n + 8 * n
+
+
+def bytes_fused_16bit(Tr, n):
+    """What the 16-bit forms must move per search: the float32 input read by the moments pass
+    and again by normalisation, the 16-bit copy written and read once by the tree, and the
+    per-channel tops and column sums: 4*Tr*N*2 + 2*Tr*N*2 + 8*N."""
+    return 12 * Tr * n + 8 * n
+
+
+def num_sms():
+    import torch
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
 
 
 def cpu_baseline(kind="reference", steps=1):
@@ -142,7 +166,7 @@ def cpu_baseline(kind="reference", steps=1):
         times.append(time.perf_counter() - t0)
     sec = float(np.median(times))
     value = spec.samples() / sec / 1e9
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "ms_per_step": sec * 1e3,
             "sample": f"1 coarse channel (16 x 2^20, {spec.num_drift_blocks()} drift blocks), "
                       f"{sec:.2f} s per search, median of {steps}"}
 
@@ -154,7 +178,8 @@ def run_reference(args, world, rank):
         pass  # the CPU path has no warm-up state beyond the first call below
     cb = cpu_baseline("reference", steps=max(1, args.steps))
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "node: 64 coarse x 16 x 2^20 float32, max_drift 4 Hz/s, snr 10 "
                                    "(CPU sample: 1 coarse channel per step)"},
@@ -199,13 +224,12 @@ def _time_pool(torch, pool, reqs, steps, warmup, stream):
     return e0.elapsed_time(e1) / steps, res
 
 
-def run_uneven(args, world, rank, local):
+def uneven_result(world, rank, local, n, steps, warmup, subsets=True):
     """Batched uneven searches through the pool (sc_dd_pool): autotuned on the first call,
     captured as CUDA graphs on the second, replayed afterwards; FP32 and BF16 storage (the
     whole mix, and the searches of 16 timesteps on their own)."""
     import torch
     from seticore_b200 import SearchPool
-    n = args.count or 512
     specs, reqs = _uneven_requests(torch, n, seed=4000 + 1000 * rank)
     samples = sum(r.input.shape[0] * r.input.shape[1] for r in reqs)
     stream = torch.cuda.current_stream()
@@ -213,13 +237,13 @@ def run_uneven(args, world, rank, local):
     barrier(world)
     clocks = Clocks(local)
     clocks.start()
-    ms, res32 = _time_pool(torch, pool, reqs, args.steps, args.warmup, stream)
+    ms, res32 = _time_pool(torch, pool, reqs, steps, warmup, stream)
     clk = clocks.stop()
     ms = max_over_ranks(ms, world)
     st = pool.stats()
     calls = max(1, st.calls)
     out = {"metric": "dedoppler Gsamples/s (FP32, 512 uneven searches)", "value": world * samples / (ms / 1e3) / 1e9,
-           "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"uneven: {n} searches, T in {{16,32,64,128,256}}, N in {{2^16,2^17,2^18,2^20}}, "
                                   "max_drift U(1,10) Hz/s, 0-6 tones SNR 12-80", "samples_per_step": samples,
@@ -231,12 +255,12 @@ def run_uneven(args, world, rank, local):
     # The searches of 16 timesteps alone, FP32 against BF16 / FP16 storage (identical hits required).
     t16 = [r for r in reqs if r.input.shape[0] <= 16]
     sub = {}
-    if t16:
+    if t16 and subsets:
         s16 = sum(r.input.shape[0] * r.input.shape[1] for r in t16)
         for prec in ["fp32", "bf16", "fp16"]:
             rq = _with_precision(t16, prec)
             p = SearchPool(scratch_budget_bytes=16 << 30)
-            m, r = _time_pool(torch, p, rq, args.steps, args.warmup, stream)
+            m, r = _time_pool(torch, p, rq, steps, warmup, stream)
             m = max_over_ranks(m, world)
             sub[prec] = {"value": world * s16 / (m / 1e3) / 1e9, "ms_per_step": m}
             if prec == "fp32":
@@ -250,24 +274,29 @@ def run_uneven(args, world, rank, local):
     # The whole mix with BF16 storage.
     rq = _with_precision(reqs, "bf16")
     p = SearchPool(scratch_budget_bytes=16 << 30)
-    m, r = _time_pool(torch, p, rq, args.steps, args.warmup, stream)
+    m, r = _time_pool(torch, p, rq, steps, warmup, stream)
     m = max_over_ranks(m, world)
     out["bf16_mix"] = {"value": world * samples / (m / 1e3) / 1e9, "ms_per_step": m,
                        "hits_identical_to_fp32": _hit_keys(r) == keys32}
     p.close()
     pool.close()
+    del reqs, rq
+    return out
+
+
+def run_uneven(args, world, rank, local):
+    out = uneven_result(world, rank, local, args.count or 512, args.steps, args.warmup)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-def run_serve(args, world, rank, local):
+def serve_result(world, rank, local, n_inputs, serve_seconds):
     """Continuous batching (seticore_b200.serving): Poisson arrivals of searches drawn from
     the uneven mix, admitted by a 120 GB HBM budget, inputs resident on the device.
     Capacity is measured first with every request submitted at once; then arrivals are
     offered at 0.5, 0.8, 1.0 and 1.2 x capacity.  Latency is arrival to result (wall clock)."""
     import torch
     from seticore_b200 import SearchPool, SearchServer, run_load
-    n_inputs = args.count or 128
     specs, reqs = _uneven_requests(torch, n_inputs, seed=5000 + 1000 * rank)
     stream = torch.cuda.current_stream()
     ref = SearchPool(scratch_budget_bytes=16 << 30)
@@ -295,7 +324,7 @@ def run_serve(args, world, rank, local):
         points = []
         for load in [0.5, 0.8, 1.0, 1.2]:
             rate = load * cap_rps
-            n_req = int(min(4 * n_inputs, max(64, rate * args.serve_seconds)))
+            n_req = int(min(4 * n_inputs, max(64, rate * serve_seconds)))
             _, lat, wall, smp = run_load(lambda i: base[i % n_inputs], n_req, rate, server, seed=int(load * 100))
             points.append({"offered_load": load, "rate_per_s": rate, "requests": n_req,
                            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
@@ -304,18 +333,23 @@ def run_serve(args, world, rank, local):
         server.close()
         out["forms"][form] = {"capacity_requests_per_s": cap_rps, "capacity_gsamples_per_s": samples / cap_s / 1e9,
                               "hits_identical_to_fp32": identical, "points": points, "server": st}
+    del reqs
+    return out
+
+
+def run_serve(args, world, rank, local):
+    out = serve_result(world, rank, local, args.count or 128, args.serve_seconds)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-def run_beams(args, world, rank, local):
+def beams_result(world, rank, local, n, steps, warmup):
     """Beamformed-style case: 64 beams x 256 timesteps x 131072 channels (foff 3.81 Hz,
     tsamp 0.268 s, max_drift 10 Hz/s), one batched call; more than 32 rows, so the
     level path runs."""
     import torch
     from seticore_b200 import Dedopplerer
     from seticore_b200.synthetic import config_beams, make_filterbank_torch
-    n = args.count or 64
     specs = config_beams(n, base_seed=3000 + 1000 * rank)
     sp = specs[0]
     data = torch.empty((n, sp.rounded_timesteps, sp.num_channels), dtype=torch.float32, device="cuda")
@@ -325,7 +359,7 @@ def run_beams(args, world, rank, local):
     dd = Dedopplerer(sp.num_timesteps, sp.num_channels, sp.foff_mhz, sp.tsamp)
     stream = torch.cuda.current_stream()
     inputs = [data[i] for i in range(n)]
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         res = dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold, stream=stream)
     barrier(world)
     torch.cuda.synchronize()
@@ -333,40 +367,54 @@ def run_beams(args, world, rank, local):
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         res = dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold, stream=stream)
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
     samples = n * sp.rounded_timesteps * sp.num_channels
     keys32 = _hit_keys(res)
     precision = {}
     for prec in ["bf16", "fp16"]:
         dd.set_precision(prec)
-        for _ in range(max(3, args.warmup)):
+        for _ in range(max(3, warmup)):
             got = dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold,
                                       stream=stream)
         torch.cuda.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             dd.search_batch_raw(inputs, list(range(n)), [0] * n, sp.max_drift, 0.0, sp.snr_threshold, stream=stream)
         p1.record(stream)
         torch.cuda.synchronize()
         st = dd.last_stats()
-        p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
+        p_ms = max_over_ranks(p0.elapsed_time(p1) / steps, world)
         precision[prec] = {"value": world * n * sp.rounded_timesteps * sp.num_channels / (p_ms / 1e3) / 1e9,
                            "ms_per_step": p_ms, "hits_identical_to_fp32": _hit_keys(got) == keys32,
                            "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}"}
     dd.set_precision("fp32")
+    peak, peak_src = measured_peak_hbm()
+    ndb = sp.num_drift_blocks()
     out = {"metric": "dedoppler Gsamples/s (FP32, 64 beams x 256 x 131072)", "value": world * samples / (ms / 1e3) / 1e9,
-           "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"beams: {n} x 256 x 131072, foff 3.81 Hz, tsamp 0.268 s, max_drift 10 Hz/s",
                       "drift_blocks": sp.num_drift_blocks(), "input_bytes": samples * 4},
-           "clocks": clk, "hits_per_step": sum(len(h) for h in res), "precision_forms": precision}
+           "clocks": clk, "hits_per_step": sum(len(h) for h in res), "precision_forms": precision,
+           "hbm": {"peak_gbs": peak, "peak_source": peak_src,
+                   "dram_bytes_per_beam": BEAMS_DRAM_BYTES,
+                   "dram_frac_of_step": n * BEAMS_DRAM_BYTES / (ms / 1e3) / 1e9 / peak,
+                   "input_read_once_frac_of_step": 4 * samples / (ms / 1e3) / 1e9 / peak,
+                   "bytes_if_read_per_drift_block_frac": n * bytes_read_per_drift_block(
+                       sp.rounded_timesteps, sp.num_channels, ndb) / (ms / 1e3) / 1e9 / peak}}
     dd.close()
+    del data, inputs
+    return out
+
+
+def run_beams(args, world, rank, local):
+    out = beams_result(world, rank, local, args.count or 64, args.steps, args.warmup)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -386,6 +434,8 @@ def main():
                     help="node (the headline line); uneven, serve and beams print their own lines")
     ap.add_argument("--count", type=int, default=0, help="searches of the uneven / serve / beams workloads")
     ap.add_argument("--serve-seconds", type=float, default=8.0, help="offered-load duration per serving point")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="node line only (by default a 1-GPU run adds the beams, uneven and serve results)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "ours" and args.workload != "node":
@@ -467,11 +517,13 @@ def main():
         barrier(world)
         st = dd.last_stats()
         p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
-        alg16 = algorithmic_bytes_16bit(T, N, specs[0].num_drift_blocks()) * n_coarse
+        alg16 = bytes_fused_16bit(T, N) * n_coarse
         peak16, _ = measured_peak_hbm()
         precision[prec] = {"value": world * samples_per_step / (p_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": p_ms,
-                           "hbm_roofline_frac_of_step": alg16 / (p_ms / 1e3) / 1e9 / peak16,
-                           "algorithmic_bytes_per_step": alg16,
+                           "hbm_frac_of_step": alg16 / (p_ms / 1e3) / 1e9 / peak16,
+                           "bytes_per_step": alg16,
+                           "bytes_per_step_note": "moments read + normalise read/write + one 16-bit tree read "
+                                                  "+ tops and column sums (12*Tr*N + 8*N per search)",
                            "hits_identical_to_fp32": identical,
                            "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}",
                            "speedup_vs_fp32": ms / p_ms}
@@ -506,11 +558,12 @@ def main():
                 if ci + 1 < len(chunks):
                     issue_copy(ci + 1)
                 stream.wait_event(done[b])
-                res = dd.search_batch_raw([bufs[b][k] for k in range(m)], [-1] * m, list(range(j, j + m)),
-                                          MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
+                dd.search_batch_raw([bufs[b][k] for k in range(m)], [-1] * m, list(range(j, j + m)),
+                                    MAX_DRIFT, MIN_DRIFT, SNR, stream=stream)
                 freed[b].record(stream)
-                # headers + first candidates of each search come back in two copies per call
-                nbytes += m * (32 + 24 * 256)
+                # the bytes the call copied device -> host (headers and candidates), as the
+                # library counted them
+                nbytes += dd.last_stats().d2h_bytes
             return nbytes
 
         for f in freed:
@@ -535,17 +588,33 @@ def main():
 
     ndb = spec0.num_drift_blocks()
     per_launch = min(n_coarse, 64)
-    alg = algorithmic_bytes_fp32(T, N, ndb) * per_launch
     # tree_ms times the one tree-kernel launch that covers the first (up to) 64 searches
     tree_launch_ms = float(np.mean(tree_ms))
     peak, peak_src = measured_peak_hbm()
+    alg = bytes_fused_fp32(T, N) * per_launch
     achieved = alg / (tree_launch_ms / 1e3) / 1e9
+    traffic = TREE_DRAM_BYTES * per_launch
+    sms = num_sms()
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    # Instruction issue: 4 warp instructions per clock per SM at the sampled SM clock.
+    issue_roof_ms = TREE_WARP_INSTR * per_launch / (sms * 4 * sm_mhz * 1e6) * 1e3
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": (TREE_DRAM_BYTES * per_launch if TREE_DRAM_BYTES else None), "peak_source": peak_src,
-                "kernel": "tree_max_kernel<float,16,1,33> (8 warps, 2 CTAs per SM, leaves reread from 12)", "searches_per_launch": per_launch,
-                "kernel_ms": tree_launch_ms, "algorithmic_bytes_per_launch": alg,
-                "note": "algorithmic bytes assume one tree read per drift block; the fused kernel stages each "
-                        "input tile once for all drift blocks, so frac > 1 is expected"}
+                "traffic": traffic, "peak_source": peak_src,
+                "kernel": "tree_max_kernel<float,16,1,33> (8 warps, 2 CTAs per SM, leaves reread from 12)",
+                "searches_per_launch": per_launch, "kernel_ms": tree_launch_ms,
+                "algorithmic_bytes_per_launch": alg,
+                "algorithmic_bytes_note": "input read once + top sums and column sums written, 4*Tr*N + 8*N "
+                                          "per search",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per coarse channel "
+                                  "(profiles/tree_max_kernel_node.md) x searches per launch",
+                "traffic_frac": traffic / (tree_launch_ms / 1e3) / 1e9 / peak,
+                "binding_limit": "instruction issue",
+                "issue_roof": {"warp_instructions_per_launch": TREE_WARP_INSTR * per_launch, "sms": sms,
+                               "sm_mhz": sm_mhz, "roof_ms": issue_roof_ms, "frac": issue_roof_ms / tree_launch_ms,
+                               "source": "ncu smsp__inst_executed.sum (profiles/tree_max_kernel_node.md)"},
+                "bytes_if_read_per_drift_block": bytes_read_per_drift_block(T, N, ndb) * per_launch,
+                "bytes_if_read_per_drift_block_note": "the reference's schedule (one input read per drift "
+                                                      "block); not a bound for the fused kernel"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -560,10 +629,26 @@ def main():
             "gpu_launches": len(tree_ms) * LAUNCHES_PER_BATCH * ((n_coarse + 63) // 64),
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline("reference", steps=1)
+        line["cpu_baseline"] = cpu_baseline("reference", steps=3)
+    dd.close()
+    if world == 1 and not args.no_extra:
+        # The other workloads, each bounded to a few seconds of timed work, as extra keys of this
+        # line: the node's buffers are released first (the uneven mix holds 71 GB of inputs).
+        inputs = data = bufs = host = None  # noqa: F841
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        extra_steps = max(1, min(args.steps, 3))
+        for key, fn in (("beams", lambda: beams_result(world, rank, local, 64, max(1, min(args.steps, 5)), 3)),
+                        ("uneven", lambda: uneven_result(world, rank, local, 512, extra_steps, 3, subsets=False)),
+                        ("serve", lambda: serve_result(world, rank, local, 64, min(args.serve_seconds, 2.0)))):
+            try:
+                line[key] = fn()
+            except Exception as exc:  # recorded, so that the headline line still prints
+                line[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    dd.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

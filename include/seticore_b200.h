@@ -49,7 +49,7 @@ typedef struct sc_dd_hit {
   int num_timesteps;      /* unrounded timesteps of the engine */
 } sc_dd_hit;
 
-/* Statistics of the last search (dedoppler.cu:322-354). */
+/* Statistics of the last search (dedoppler.cu:242-273). */
 typedef struct sc_dd_stats {
   float median;
   float std_dev;
@@ -64,7 +64,7 @@ typedef struct sc_dd_stats {
   int precision;          /* SC_DD_PRECISION_* of the search */
   int recomputed_channels; /* precision form: channels whose top was recomputed in FP32 */
   int total_channels;      /* channels of the search */
-  int pad;
+  int d2h_bytes;           /* bytes the whole call copied device -> host (headers, candidates) */
   double norm_mean;       /* precision form: FP64 mean of the power, used to normalise */
   double norm_std;        /* precision form: FP64 standard deviation, used to normalise */
 } sc_dd_stats;
@@ -144,6 +144,14 @@ const char* sc_dd_last_error(void);
 
 /* Library version string. */
 const char* sc_dd_version(void);
+
+/* Test hook, no counterpart in the reference.  Every tree launch queued after this call
+ * polls the mbarrier of its staged rows at most `tries` times before it gives up (tries < 0
+ * restores the default, about a second).  A CTA that gives up waits for its copies to land
+ * and leaves, and the search reports SC_DD_EINTERNAL.  With 0, every search whose tree
+ * stages rows by bulk copies gives up: the tests use this to exercise the give-up path
+ * without a fault.  Process-wide; a CUDA graph keeps the limit it was captured with. */
+int sc_dd_set_stage_wait_limit(int tries);
 
 /* The device half of H5Reader::loadCoarseChannel (h5_reader.cpp:190-209) for `count`
  * coarse channels laid out item_stride floats apart, each [rounded_timesteps][row_stride]:
@@ -230,14 +238,16 @@ const char* sc_dd_pool_last_error(void);
  * is one fixed device array inside the library (about 10.1 MB, held by every GPU that loads
  * the library until the process exits) and its host side uses the stack and `out`.
  * Limits (SC_DD_ELIMIT beyond them): num_channels <= SC_DD_STATIC_MAX_CHANNELS, rounded
- * timesteps <= 16, at most 65536 windows (num_channels / window_size).  Errors are status
+ * timesteps <= 16, at most 65536 windows (num_channels / window_size).  A max_drift that is
+ * not finite, or whose drift range exceeds sc_dd_search's bound, is SC_DD_EINVAL.  Errors are status
  * codes only (sc_dd_last_error is not updated).
  *
  * The array is shared by every call on a device and keeps the last call's contents; each
  * call clears what must start at zero.  Calls that overlap on the GPU -- on different
  * streams, or from different host threads -- race on it and must be serialised by the
  * caller.  The first call on each device looks up the array's device address (with that
- * device current) and caches it; make that first call before any stream capture.  On
+ * device current) and caches it; make that first call before any stream capture.  Every
+ * call copies its results to the host and synchronizes `stream` before it returns.  On
  * SC_DD_ETRUNC, *num_hits is the total and the hits written are not necessarily the
  * lowest-index ones. */
 int sc_dd_search_static(const float* dev_input, long long row_stride, int num_timesteps,

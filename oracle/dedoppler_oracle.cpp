@@ -204,13 +204,13 @@ int oracle_search(const float* input, int Tr, int N, double foff, double tsamp,
                   oracle_hit* hits, int cap, float* top_sums_out, int* top_db_out,
                   int* top_off_out, float* colsums_out, oracle_stats* stats) {
   const int drift_timesteps = Tr - 1;                                   // dedoppler.cu:165
-  const double res = 1e6 * foff / (drift_timesteps * tsamp);            // dedoppler.cu:167
-  const double diag = res * drift_timesteps;                            // dedoppler.cu:275
-  const double nmax = max_drift / std::abs(diag);                       // dedoppler.cu:276
+  const double res = 1e6 * foff / (drift_timesteps * tsamp);            // dedoppler.cu:87
+  const double diag = res * drift_timesteps;                            // dedoppler.cu:195
+  const double nmax = max_drift / std::abs(diag);                       // dedoppler.cu:196
   const int dmin = (int)std::floor(-nmax);
   const int dmax = (int)std::floor(nmax);
 
-  // sumColumns (dedoppler.cu:143-152): sequential float sum in row order.
+  // sumColumns (dedoppler.cu:63-72): sequential float sum in row order.
   std::vector<float> colsum(N);
   for (int c = 0; c < N; ++c) {
     float s = 0.0f;
@@ -218,7 +218,7 @@ int oracle_search(const float* input, int Tr, int N, double foff, double tsamp,
     colsum[c] = s;
   }
 
-  // findTopPathSums (dedoppler.cu:112-135), top sums reset to 0 (dedoppler.cu:285).
+  // findTopPathSums (dedoppler.cu:32-55), top sums reset to 0 (dedoppler.cu:205).
   std::vector<float> top(N, 0.0f);
   std::vector<int> topdb(N, 0), topoff(N, 0);
   std::vector<float> b1((size_t)Tr * N), b2((size_t)Tr * N);
@@ -228,7 +228,7 @@ int oracle_search(const float* input, int Tr, int N, double foff, double tsamp,
     for (int c = 0; c < N; ++c) {
       for (int off = 0; off < Tr; ++off) {
         const long last = (long)(Tr - 1) * db + off + c;
-        if (last < 0 || last >= N) break;  // early return, dedoppler.cu:122-126
+        if (last < 0 || last >= N) break;  // early return, dedoppler.cu:40-46
         const float v = sums[(size_t)off * N + c];
         if (v > top[c]) {
           top[c] = v;
@@ -239,7 +239,7 @@ int oracle_search(const float* input, int Tr, int N, double foff, double tsamp,
     }
   }
 
-  // Host statistics (dedoppler.cu:325-342), same library calls in the same order.
+  // Host statistics (dedoppler.cu:242-262), same library calls in the same order.
   std::vector<float> cs(colsum);
   const int mid = N / 2;
   std::nth_element(cs.begin(), cs.begin() + mid, cs.end());
@@ -255,7 +255,7 @@ int oracle_search(const float* input, int Tr, int N, double foff, double tsamp,
                 [&](const float f) { accum += (f - m) * (f - m); });
   const float std_dev = std::sqrt(accum / (last + 1 - first));
 
-  // Window de-duplication (dedoppler.cu:353-399).
+  // Window de-duplication (dedoppler.cu:264-319).
   const float thr = snr_threshold * std_dev + median;
   const int window_size = 2 * std::ceil(nmax * drift_timesteps);
   if (stats) {

@@ -13,6 +13,7 @@
 // in two copies and synchronises once.  Only hit lists cross to the host, not the
 // reference's four N-length arrays per search.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -65,7 +66,7 @@ struct DeviceGuard {
   }
 };
 
-// The drift range and window of a search (dedoppler.cu:165-167, 274-278, 354).
+// The drift range and window of a search (dedoppler.cu:84-87, 194-198, 274).
 struct DriftPlan {
   double res;
   int dmin, dmax, window_size;
@@ -334,6 +335,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
   cudaError_t e;
   if ((e = cudaEventRecord(dd->ev[0], stream)) != cudaSuccess) return cuda_fail(e, "event");
   int total = 0;
+  long long d2h = 0;
   for (int k0 = 0; k0 < count; k0 += scb::kMaxBatch) {
     const int n = std::min(scb::kMaxBatch, count - k0);
     rc = queue_batch(dd, n, inputs + k0, strides + k0, p, snr_threshold, stream, k0 == 0);
@@ -353,6 +355,8 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
                               cudaMemcpyDeviceToHost, stream)) != cudaSuccess) ||
         (e = cudaStreamSynchronize(stream)) != cudaSuccess)
       return cuda_fail(e, "result copy");
+    d2h += (long long)(sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * head) * n +
+           (prec ? (long long)sizeof(int) * n + (k0 == 0 ? 2 * (long long)sizeof(double) : 0) : 0);
     for (int k = 0; k < n; ++k) {
       const scb::SearchHeader h = dd->host_hdrs()[k];
       if (h.error) return fail(SC_DD_EINTERNAL, "a tree kernel gave up waiting for its staged rows");
@@ -366,6 +370,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
                 cudaSuccess ||
             (e = cudaStreamSynchronize(stream)) != cudaSuccess)
           return cuda_fail(e, "candidate copy");
+        d2h += (long long)sizeof(scb::Candidate) * (ncand - head);
       }
       std::sort(cands.begin(), cands.end(),
                 [](const scb::Candidate& a, const scb::Candidate& b) { return a.index < b.index; });
@@ -389,7 +394,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
         int drift_bins = 0;
         if (!scb::decode_candidate(c, p.dmin, Tr, &drift_bins))
           return fail(SC_DD_EINTERNAL, "drift recovery did not reproduce a top sum");
-        // dedoppler.cu:385-396
+        // dedoppler.cu:305-317
         const double drift_rate = drift_bins * p.res;
         const float snr = (c.power - h.median) / h.std_dev;
         if (std::fabs(drift_rate) >= min_drift) {
@@ -412,6 +417,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
       num_hits[k0 + k] = nk;
     }
   }
+  dd->last.d2h_bytes = (int)std::min<long long>(d2h, INT_MAX);
   cudaEventElapsedTime(&dd->last.tree_ms, dd->ev[1], dd->ev[2]);
   cudaEventElapsedTime(&dd->last.search_ms, dd->ev[0], dd->ev[3]);
   dd->have_last = true;
@@ -426,6 +432,11 @@ extern "C" {
 const char* sc_dd_last_error(void) { return g_last_error.c_str(); }
 
 const char* sc_dd_version(void) { return "seticore-b200 0.2 (dedoppler; reference seticore 1.0.6)"; }
+
+int sc_dd_set_stage_wait_limit(int tries) {
+  scb::set_stage_wait_tries(tries);
+  return SC_DD_OK;
+}
 
 int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double tsamp_s, int has_dc_spike,
                  sc_dd** out) {

@@ -45,9 +45,9 @@ SearchDesc to_desc(const ExecSearch& e) {
   s.dmin = e.dmin;
   s.dmax = e.dmax;
   s.window_size = e.window_size;
-  s.first = (int)ceil(0.05 * e.N);  // dedoppler.cu:327
-  s.mid = e.N / 2;                   // dedoppler.cu:291
-  s.last = (int)floor(0.95 * e.N);  // dedoppler.cu:328
+  s.first = (int)ceil(0.05 * e.N);  // dedoppler.cu:247
+  s.mid = e.N / 2;                   // dedoppler.cu:211
+  s.last = (int)floor(0.95 * e.N);  // dedoppler.cu:248
   s.snr_threshold = e.snr_threshold;
   s.top = e.top;
   s.colsum = e.colsum;

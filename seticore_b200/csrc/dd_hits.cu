@@ -1,6 +1,6 @@
 // Hit selection on the GPU.
 //
-// window_kernel: the reference's window de-duplication (dedoppler.cu:353-383).  Channels
+// window_kernel: the reference's window de-duplication (dedoppler.cu:264-303).  Channels
 //   are cut into non-overlapping windows of window_size; a window's candidate is the
 //   first channel holding its largest top sum, if that sum is strictly above the
 //   threshold; it survives if no channel in [c - window_size + 1, c + window_size) has a

@@ -151,8 +151,17 @@ struct TreeGroup {
 struct TreeBatch {
   int count;
   int n_items;
+  // Polls of the staging wait before a CTA gives up (negative: the default, about a second).
+  // The launcher fills it from stage_wait_tries().
+  int stage_wait_tries = -1;
   TreeGroup g[kMaxBatch];
 };
+
+// The staging-wait poll limit of tree launches queued from now on (negative: the default).
+// Tests set 0 to make every staged item give up, which exercises the give-up path (the
+// search then reports SC_DD_EINTERNAL) without any fault.
+void set_stage_wait_tries(int tries);
+int stage_wait_tries();
 
 // Launch shape of a tree launch.  smem_kb bounds the shared memory of a CTA (0: the
 // default), which sets how many drift blocks share a staged trapezoid and how many CTAs fit
@@ -224,7 +233,7 @@ cudaError_t column_sums_batch(const SearchBatch& b, cudaStream_t stream);
 // sums and a reset select state (column_sums_batch or exec_queue's clear launch).
 cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
 
-// Window de-duplication (dedoppler.cu:353-383) and drift recovery of the survivors.
+// Window de-duplication (dedoppler.cu:264-303) and drift recovery of the survivors.
 cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
 
 // Path sums along the given (index, drift_steps) paths: addIncoherentPower.

@@ -96,15 +96,20 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
     return fail(SC_DD_EINVAL, "sc_dd_search_static: foff must be nonzero and tsamp positive");
   const int N = num_channels;
 
-  // dedoppler.cu:165-167, 274-278, 354: the same double arithmetic as sc_dd_search.
+  // dedoppler.cu:84-87, 194-198, 274: the same double arithmetic as sc_dd_search.
   const int drift_timesteps = Tr - 1;
   const double res = 1e6 * foff_mhz / (drift_timesteps * tsamp_s);
   const double nmax = max_drift / std::fabs(res * drift_timesteps);
+  // The same bound on the drift range as sc_dd_search, checked before any int conversion.
+  if (!std::isfinite(max_drift) || !std::isfinite(nmax) || nmax * drift_timesteps > (double)(1 << 30))
+    return fail(SC_DD_EINVAL, "sc_dd_search_static: max_drift is not finite or too large");
   const int dmin = (int)std::floor(-nmax);
   const int dmax = (int)std::floor(nmax);
   const int window_size = (int)(2 * std::ceil(nmax * drift_timesteps));
   if (!(window_size >= 1) || dmax < dmin)
     return fail(SC_DD_EINVAL, "sc_dd_search_static: max_drift gives no drift range (window size < 1)");
+  if ((long long)(dmax - dmin + 1) * Tr > (1ll << 30))
+    return fail(SC_DD_EINVAL, "sc_dd_search_static: drift range too large");
   if ((long long)(N + window_size - 1) / window_size > kStaticMaxCands)
     return fail(SC_DD_ELIMIT, "sc_dd_search_static: more than 65536 windows; use sc_dd_search");
 
@@ -203,7 +208,7 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
       int drift_steps = 0;
       if (!scb::decode_candidate(c, dmin, Tr, &drift_steps))
         return fail(SC_DD_EINTERNAL, "sc_dd_search_static: drift recovery did not reproduce a top sum");
-      const double drift_rate = drift_steps * res;  // dedoppler.cu:385-396
+      const double drift_rate = drift_steps * res;  // dedoppler.cu:305-317
       const float snr = (c.power - h.median) / h.std_dev;
       if (std::fabs(drift_rate) >= min_drift) {
         if (n < capacity) {

@@ -387,7 +387,7 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
     q.T = r.num_timesteps;
     q.Tr = round_up_pow2(r.num_timesteps);
     q.N = r.num_channels;
-    // dedoppler.cu:165-167, 274-278, 354
+    // dedoppler.cu:84-87, 194-198, 274
     const int dt = q.Tr - 1;
     pl.res = 1e6 * r.foff_mhz / (dt * r.tsamp_s);
     const double nmax = r.max_drift / std::fabs(pl.res * dt);
@@ -516,7 +516,7 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
         int drift_bins = 0;
         if (!scb::decode_candidate(c, pl.es.dmin, pl.es.Tr, &drift_bins))
           return pfail(SC_DD_EINTERNAL, "drift recovery did not reproduce a top sum");
-        const double drift_rate = drift_bins * pl.res;  // dedoppler.cu:385-396
+        const double drift_rate = drift_bins * pl.res;  // dedoppler.cu:305-317
         const float snr = (c.power - hd.median) / hd.std_dev;
         if (std::fabs(drift_rate) >= pl.min_drift) {
           if (total < capacity) {

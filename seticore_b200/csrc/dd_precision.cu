@@ -17,7 +17,7 @@
 //      floored at 0, becomes its top.  Every other channel keeps top 0:
 //      its approximate top is below 0.9 x threshold, so its exact top is below the
 //      threshold and it can neither become a window candidate nor beat one
-//      (dedoppler.cu:353-383 compares only with values above the threshold).  The hit list
+//      (dedoppler.cu:275-302 compares only with values above the threshold).  The hit list
 //      is therefore the plain form's.
 // The statistics (median, standard deviation, threshold) always come from the float32
 // column sums, exactly as in the plain form.

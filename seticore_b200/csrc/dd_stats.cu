@@ -2,7 +2,7 @@
 //
 // The reference copies the column sums to the host and uses std::nth_element for the
 // median and the 5% / 95% order statistics, then a mean and standard deviation over the
-// sorted positions [ceil(0.05 N), floor(0.95 N)] (dedoppler.cu:322-342).  Here:
+// sorted positions [ceil(0.05 N), floor(0.95 N)] (dedoppler.cu:242-262).  Here:
 //   * colsum_kernel: sumColumns (dedoppler.cu:63-72), same sequential float order.
 //   * range_kernel, hist_kernel (x3), compact_kernel, select_finish_kernel: the three order
 //     statistics at once.  The key range [kmin, kmax] is cut into 4096 bins; the bin holding
@@ -14,7 +14,7 @@
 //     percentiles' ranges; the finaliser adds the boundary candidates and ties exactly and
 //     forms the mean with the reference's roundings (float sum, float division).
 //   * var_chunk_kernel + var_emulate_kernel: the variance.  The reference accumulates
-//     (f - m)^2 in FLOAT, one term at a time (dedoppler.cu:337-341).  Once the
+//     (f - m)^2 in FLOAT, one term at a time (dedoppler.cu:257-261).  Once the
 //     accumulator is large, every term is rounded to the accumulator's ulp and terms
 //     under half an ulp vanish, which biases the sum low (about 4e-4 relative at 2^20
 //     channels, nearly independent of the order).  An exact FP64 variance would
@@ -367,7 +367,7 @@ __device__ void sort_keys(uint32_t* k, int n) {
 }
 
 // One CTA per search: the exact order statistics from the collected candidates, then the
-// mean over the sorted positions [first, last] as the reference forms it (dedoppler.cu:322-336):
+// mean over the sorted positions [first, last] as the reference forms it (dedoppler.cu:255-256):
 // a double sum of the floats, rounded to float, divided by the count in float.
 __global__ void __launch_bounds__(kSelThreads) select_finish_kernel(const __grid_constant__ SearchBatch b,
                                                                     int n_partials) {
@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(kSelThreads) select_finish_kernel(const __grid
     s1 = inner + (double)n_lo * v_first + (double)n_hi * v_last;
   }
   const float sum_f = (float)s1;
-  const float m = sum_f / (float)n;  // dedoppler.cu:335-336: float sum / count
+  const float m = sum_f / (float)n;  // dedoppler.cu:255-256: float sum / count
   hdr->median = v_mid;
   hdr->mean = m;
   st->mean = m;
@@ -658,9 +658,9 @@ __global__ void var_emulate_kernel(const __grid_constant__ SearchBatch b) {
   }
   st->ticket = 0;
   const float accum_f = (float)acc;
-  const float std_dev = sqrtf(accum_f / (float)st->n);  // dedoppler.cu:342
+  const float std_dev = sqrtf(accum_f / (float)st->n);  // dedoppler.cu:262
   hdr->std_dev = std_dev;
-  hdr->threshold = (float)(snr_threshold * (double)std_dev + (double)hdr->median);  // dedoppler.cu:353
+  hdr->threshold = (float)(snr_threshold * (double)std_dev + (double)hdr->median);  // dedoppler.cu:273
 }
 
 }  // namespace

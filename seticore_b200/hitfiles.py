@@ -4,7 +4,7 @@
   * HitFileWriter      -- hit_file_writer.cpp:18-97 (one Hit message per hit, written to
                           <name>.tmp and renamed on close; each carries the hit's Signal and a
                           Filterbank slice of the input, 40 extra columns either side)
-  * makeHitRecorder    -- hit_recorder.cpp:10-24 (chooses by file suffix)
+  * makeHitRecorder    -- hit_recorder.cpp:10-23 (chooses by file suffix)
   * read_hits          -- what hitls.cpp reads: the Hit messages of a .hits file
 
 The Cap'n Proto encoding is written here from the published wire format (no capnp library
@@ -385,7 +385,7 @@ class HitFileWriter(HitRecorder):
 
 
 def makeHitRecorder(filename: str, metadata, max_drift: float) -> HitRecorder:
-    """hit_recorder.cpp:10-24."""
+    """hit_recorder.cpp:10-23."""
     if filename.endswith(".dat"):
         return DatFileWriter(filename, metadata, max_drift)
     if filename.endswith(".hits"):

@@ -1,6 +1,6 @@
 """End to end: a filterbank file to a hit file (run_dedoppler.cpp:30-53).
 
-  * FilterbankFileReader / loadFilterbankFile -- filterbank_file_reader.cpp:10-30
+  * FilterbankFileReader / loadFilterbankFile -- filterbank_file_reader.cpp:11-28
   * FilReader            -- fil_reader.cpp:16-139 (sigproc header); its loadCoarseChannel,
                             a stub in the reference (fil_reader.cpp:151-154), reads the
                             coarse channel's columns of every row here
@@ -201,7 +201,7 @@ def write_fil(filename: str, data: np.ndarray, metadata: FilterbankMetadata) -> 
 
 
 def loadFilterbankFile(filename: str) -> FilterbankFileReader:
-    """filterbank_file_reader.cpp:16-30."""
+    """filterbank_file_reader.cpp:17-28."""
     if filename.endswith(".h5"):
         raise RuntimeError(f"{filename}: HDF5 filterbank files need libhdf5, which this package does not link")
     if filename.endswith(".fil"):

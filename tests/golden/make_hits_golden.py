@@ -1,6 +1,7 @@
 """Generates tests/golden/voyager_hits.npz from the reference's own .hits file.
 
-Run where the reference tree exists: `python tests/golden/make_hits_golden.py`.  The
+Run where the reference tree exists (`REF=<tree> python tests/golden/make_hits_golden.py`;
+REF defaults to oracle/Makefile's).  The
 reference ships data/voyager.hits, written by its HitFileWriter (hit_file_writer.cpp) with
 an earlier hit.capnp in which Signal had 4 data words and Filterbank 8 (the fields that
 later versions appended read as zero).  The fixture keeps, per message, the sha256 of the
@@ -18,7 +19,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 from seticore_b200.hitfiles import decode_hit, split_messages  # noqa: E402
 
-SRC = "/root/reference/data/voyager.hits"
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+from conftest import reference_root  # noqa: E402  ($REF, else oracle/Makefile's default)
+
+SRC = os.path.join(reference_root(), "data", "voyager.hits")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "voyager_hits.npz")
 
 

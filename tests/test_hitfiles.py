@@ -31,7 +31,8 @@ def test_encoder_reproduces_reference_hits_file_bytes():
 
 
 def test_reference_hits_file_decodes_when_present():
-    path = "/root/reference/data/voyager.hits"
+    from conftest import reference_root
+    path = os.path.join(reference_root(), "data", "voyager.hits")
     if not os.path.exists(path):
         pytest.skip("reference tree not present")
     hits = read_hits(path)
