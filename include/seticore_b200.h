@@ -67,6 +67,14 @@ typedef struct sc_dd_stats {
   int d2h_bytes;           /* bytes the whole call copied device -> host (headers, candidates) */
   double norm_mean;       /* precision form: FP64 mean of the power, used to normalise */
   double norm_std;        /* precision form: FP64 standard deviation, used to normalise */
+  int order_exact;        /* 1: median, mean and std_dev were formed in the order the
+                             reference's std::nth_element calls leave the column sums, so they
+                             are bit-identical to the reference's (searches whose order
+                             statistics sit on repeated column-sum values, or every search
+                             after sc_dd_set_exact_statistics(1)); 0: median and mean exact,
+                             the float variance emulated in channel order (std_dev within
+                             about 1e-5 relative of the reference's on distinct values) */
+  int pad2;
 } sc_dd_stats;
 
 /* Storage of the spectra the tree reads.  FP32: the input as given (the reference's
@@ -152,6 +160,16 @@ const char* sc_dd_version(void);
  * stages rows by bulk copies gives up: the tests use this to exercise the give-up path
  * without a fault.  Process-wide; a CUDA graph keeps the limit it was captured with. */
 int sc_dd_set_stage_wait_limit(int tries);
+
+/* No counterpart in the reference (which always forms its statistics in one order).
+ * mode 0 (the default): searches whose column sums put repeated values at the 5 %, 50 % or
+ * 95 % order statistics -- integer-valued power, where the order of the reference's float
+ * variance sum moves it by up to a few 1e-4 -- get the statistics in the reference's own
+ * std::nth_element order, bit-identical; the others emulate the float sum in channel order
+ * (within about 1e-5).  mode 1: every search takes the exact order (about 4 ms per batch of
+ * up to 64 searches of 2^20 channels, one CTA per search).  Process-wide; launches queued
+ * after the call follow it (a CUDA graph keeps the mode it was captured with). */
+int sc_dd_set_exact_statistics(int mode);
 
 /* The device half of H5Reader::loadCoarseChannel (h5_reader.cpp:190-209) for `count`
  * coarse channels laid out item_stride floats apart, each [rounded_timesteps][row_stride]:

@@ -33,6 +33,7 @@ EXPORTED = [
     "sc_dd_pool_create", "sc_dd_pool_destroy", "sc_dd_pool_configure", "sc_dd_pool_search",
     "sc_dd_pool_stats_get", "sc_dd_request_scratch_bytes", "sc_dd_pool_last_error",
     "sc_dd_prepare_coarse_channels", "sc_dd_gather_columns", "sc_dd_set_stage_wait_limit",
+    "sc_dd_set_exact_statistics",
 ]
 
 
@@ -98,6 +99,8 @@ class ScDdStats(ctypes.Structure):
         ("d2h_bytes", ctypes.c_int),
         ("norm_mean", ctypes.c_double),
         ("norm_std", ctypes.c_double),
+        ("order_exact", ctypes.c_int),
+        ("pad2", ctypes.c_int),
     ]
 
 
@@ -146,6 +149,7 @@ def lib():
         L.sc_dd_prepare_coarse_channels.argtypes = [vp, i, ll, ll, i, i, i, i, vp]
         L.sc_dd_gather_columns.argtypes = [vp, ll, i, i, vp, vp, i, vp, vp]
         L.sc_dd_set_stage_wait_limit.argtypes = [i]
+        L.sc_dd_set_exact_statistics.argtypes = [i]
         L.sc_dd_last_error.restype = ctypes.c_char_p
         L.sc_dd_version.restype = ctypes.c_char_p
         for name in EXPORTED:

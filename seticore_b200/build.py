@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libseticore_b200.so")
-SOURCES = ["dd_api.cu", "dd_tree.cu", "dd_stats.cu", "dd_hits.cu", "dd_levels.cu", "dd_noalloc.cu", "dd_precision.cu",
+SOURCES = ["dd_api.cu", "dd_tree.cu", "dd_stats.cu", "dd_order.cu", "dd_hits.cu", "dd_levels.cu", "dd_noalloc.cu", "dd_precision.cu",
            "dd_exec.cu",
            "dd_pool.cu", "dd_io.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

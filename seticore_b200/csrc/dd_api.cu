@@ -100,6 +100,8 @@ struct sc_dd {
   scb::SelectState* sel = nullptr;
   scb::MomentPartial* partials = nullptr;
   double* var = nullptr;
+  float* work = nullptr;  // [slot][order_work_floats(N)] column sums in nth_element order
+  int* lists = nullptr;   // [slot][order_list_entries(N)] partition pairs
   scb::SearchHeader* hdrs = nullptr;
   scb::Candidate* cands = nullptr;
   float* scratch_a = nullptr;  // Tr > 32 level buffers (one search at a time), one allocation
@@ -156,6 +158,8 @@ void free_slots(sc_dd* d) {
   dfree(d, &d->sel, sizeof(scb::SelectState) * S);
   dfree(d, &d->partials, sizeof(scb::MomentPartial) * d->n_partials * S);
   dfree(d, &d->var, sizeof(double) * 2 * scb::kVarChunks * S);
+  dfree(d, &d->work, sizeof(float) * scb::order_work_floats(d->N) * S);
+  dfree(d, &d->lists, sizeof(int) * scb::order_list_entries(d->N) * S);
   dfree(d, &d->hdrs, sizeof(scb::SearchHeader) * S);
   dfree(d, &d->cands, sizeof(scb::Candidate) * d->cand_cap * S);
   if (d->host) cudaFreeHost(d->host);
@@ -229,6 +233,8 @@ int ensure_slots(sc_dd* d, int slots, int cand_cap) {
       (e = dalloc(d, &d->sel, sizeof(scb::SelectState) * S)) != cudaSuccess ||
       (e = dalloc(d, &d->partials, sizeof(scb::MomentPartial) * d->n_partials * S)) != cudaSuccess ||
       (e = dalloc(d, &d->var, sizeof(double) * 2 * scb::kVarChunks * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->work, sizeof(float) * scb::order_work_floats(d->N) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->lists, sizeof(int) * scb::order_list_entries(d->N) * S)) != cudaSuccess ||
       (e = dalloc(d, &d->hdrs, sizeof(scb::SearchHeader) * S)) != cudaSuccess ||
       (e = dalloc(d, &d->cands, sizeof(scb::Candidate) * (size_t)nc * S)) != cudaSuccess ||
       (e = cudaMallocHost(&d->host, (sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands) * S)) !=
@@ -291,6 +297,8 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
     q.sel = dd->sel + k;
     q.partials = dd->partials + (size_t)dd->n_partials * k;
     q.var = dd->var + (size_t)2 * scb::kVarChunks * k;
+    q.work = dd->work + scb::order_work_floats(dd->N) * k;
+    q.lists = dd->lists + scb::order_list_entries(dd->N) * k;
     q.hdr = dd->hdrs + k;
     q.cands = dd->cands + (size_t)dd->cand_cap * k;
     if (prec) {
@@ -388,6 +396,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
         dd->last.recomputed_channels = prec ? dd->host_flag_counts[0] : N;
         dd->last.norm_mean = prec ? dd->host_norm[0] : 0.0;
         dd->last.norm_std = prec ? dd->host_norm[1] : 0.0;
+        dd->last.order_exact = h.order_exact;
       }
       int nk = 0;
       for (const scb::Candidate& c : cands) {
@@ -435,6 +444,12 @@ const char* sc_dd_version(void) { return "seticore-b200 0.2 (dedoppler; referenc
 
 int sc_dd_set_stage_wait_limit(int tries) {
   scb::set_stage_wait_tries(tries);
+  return SC_DD_OK;
+}
+
+int sc_dd_set_exact_statistics(int mode) {
+  if (mode != 0 && mode != 1) return fail(SC_DD_EINVAL, "sc_dd_set_exact_statistics: mode must be 0 or 1");
+  scb::set_exact_statistics_always(mode == 1);
   return SC_DD_OK;
 }
 

@@ -54,6 +54,8 @@ SearchDesc to_desc(const ExecSearch& e) {
   s.sel = e.sel;
   s.partials = e.partials;
   s.var = e.var;
+  s.work = e.work;
+  s.lists = e.lists;
   s.hdr = e.hdr;
   s.cands = e.cands;
   s.cand_cap = e.cand_cap;
@@ -237,7 +239,8 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
 size_t ExecSearch::scratch_bytes(int Tr, int N, int cand_cap, int n_partials, int elem) {
   auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
   size_t b = a(sizeof(float) * N) * 2 + a(sizeof(SelectState)) + a(sizeof(MomentPartial) * n_partials) +
-             a(sizeof(double) * 2 * kVarChunks) + a(sizeof(SearchHeader)) + a(sizeof(Candidate) * cand_cap);
+             a(sizeof(double) * 2 * kVarChunks) + a(sizeof(float) * order_work_floats(N)) +
+             a(sizeof(int) * order_list_entries(N)) + a(sizeof(SearchHeader)) + a(sizeof(Candidate) * cand_cap);
   if (elem != kElemF32) {
     b += a((size_t)2 * Tr * N) + a(sizeof(float) * N) + a(sizeof(int) * N) + a(sizeof(int)) +
          a(sizeof(double) * (2 * kVarChunks + 2)) + a(sizeof(unsigned));
@@ -258,6 +261,10 @@ void ExecSearch::carve(char* base, int n_partials) {
   p += a(sizeof(MomentPartial) * n_partials);
   var = reinterpret_cast<double*>(p);
   p += a(sizeof(double) * 2 * kVarChunks);
+  work = reinterpret_cast<float*>(p);
+  p += a(sizeof(float) * order_work_floats(N));
+  lists = reinterpret_cast<int*>(p);
+  p += a(sizeof(int) * order_list_entries(N));
   hdr = reinterpret_cast<SearchHeader*>(p);
   p += a(sizeof(SearchHeader));
   cands = reinterpret_cast<Candidate*>(p);

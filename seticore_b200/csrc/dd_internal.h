@@ -82,7 +82,8 @@ struct Candidate {
 struct SearchHeader {
   int num_candidates;
   int error;  // nonzero: a kernel of the search gave up a wait (the results are invalid)
-  int pad0, pad1;
+  int order_exact;  // 1: the statistics were formed in the reference's nth_element order
+  int ties;         // most copies of one value among the three order statistics' values
   float median, std_dev, mean, threshold;
 };
 
@@ -99,6 +100,8 @@ struct SearchDesc {
   SelectState* sel;
   MomentPartial* partials;  // at least as many as the statistics grid's x dimension
   double* var;              // 2 * kVarChunks
+  float* work;              // order_work_floats(N): the column sums in nth_element order
+  int* lists;               // order_list_entries(N): the swap pairs of a partition step
   SearchHeader* hdr;
   Candidate* cands;
   int cand_cap;
@@ -230,8 +233,46 @@ cudaError_t recompute_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
 // each search's order-statistic state.
 cudaError_t column_sums_batch(const SearchBatch& b, cudaStream_t stream);
 // Order statistics, mean, standard deviation and threshold of each search, from its column
-// sums and a reset select state (column_sums_batch or exec_queue's clear launch).
+// sums and a reset select state (column_sums_batch or exec_queue's clear launch): the
+// order statistics exactly and the float variance emulated in channel order (dd_stats.cu),
+// then, for the searches whose order statistics sit on repeated values, everything again
+// in the reference's own nth_element order, bit-identical (dd_order.cu).
 cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
+cudaError_t search_stats_emulated(const SearchBatch& b, int num_sms, cudaStream_t stream);
+cudaError_t search_stats_exact(const SearchBatch& b, int num_sms, cudaStream_t stream);
+// The exact statistics run for a search whose three order statistics' values include one
+// held by at least this many column sums (automatic mode), or for every search.
+constexpr int kExactStatsTies = 8;
+void set_exact_statistics_always(bool always);
+bool exact_statistics_always();
+// Scratch of the exact statistics per search of N channels: the work array (N floats,
+// padded so that 16-byte loads of a range's last group stay inside it) and the pair lists
+// (two halves, one per end of the array, for the two nth_element calls that run side by side).
+#ifdef __CUDACC__
+#define SCB_HD __host__ __device__
+#else
+#define SCB_HD
+#endif
+SCB_HD constexpr size_t order_work_floats(int N) { return ((size_t)N + 7) & ~(size_t)3; }
+// One std::nth_element call of the exact statistics while its range is partitioned by
+// multi-CTA rounds (dd_order.cu); three per search, after the pair lists.
+constexpr int kOrderMaxSegs = 2048;  // counting segments of one partition step
+struct OrderTask {
+  int first, last, nth, depth;  // the call's current range, its target and depth budget
+  int sfirst, slast;            // the range of the partition step in progress
+  int active;                   // 1: the rounds partition this call; 0: its finisher does the rest
+  int error;
+  int K, cut, lk, rk;           // pairs, cut, K-th value >= pivot, (K-1)-th value <= pivot
+  unsigned ticket;              // CTAs of a round done so far
+  float pivot;
+  int nseg, seglen;
+  int seg_ge[kOrderMaxSegs + 1];  // per segment: values >= pivot, then the exclusive prefix
+  int seg_le[kOrderMaxSegs + 1];
+};
+SCB_HD constexpr size_t order_pair_entries(int N) { return 8 * ((size_t)N / 4 + 2); }
+SCB_HD constexpr size_t order_list_entries(int N) {
+  return order_pair_entries(N) + 3 * (sizeof(OrderTask) / sizeof(int)) + 64;
+}
 
 // Window de-duplication (dedoppler.cu:264-303) and drift recovery of the survivors.
 cudaError_t search_hits_batch(const SearchBatch& b, int num_sms, cudaStream_t stream);
@@ -277,6 +318,8 @@ struct ExecSearch {
   SelectState* sel;
   MomentPartial* partials;
   double* var;
+  float* work;
+  int* lists;
   SearchHeader* hdr;
   Candidate* cands;
   void* norm16;

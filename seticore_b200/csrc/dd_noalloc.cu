@@ -5,7 +5,8 @@
 // call cudaMalloc (which can synchronise the device) inside its processing loop, or a
 // host framework whose allocator owns all device memory.  This entry point serves them.
 // It runs the same kernels as sc_dd_search, but its scratch (top path sums, column sums,
-// order-statistic state, variance partials and the candidate block) lives in the
+// order-statistic state, variance partials, the exact statistics' work array and pair
+// lists, and the candidate block) lives in the
 // fixed-size device array below instead of an engine's cudaMalloc'd buffers, and its
 // host side allocates nothing either: the statistics and candidates come back through a
 // small stack buffer, and the hits are written straight into the caller's array.
@@ -38,7 +39,9 @@ constexpr size_t kOffColsum = kOffTop + align256(sizeof(float) * kStaticMaxChann
 constexpr size_t kOffSelect = kOffColsum + align256(sizeof(float) * kStaticMaxChannels);
 constexpr size_t kOffPartials = kOffSelect + align256(sizeof(scb::SelectState));
 constexpr size_t kOffVar = kOffPartials + align256(sizeof(scb::MomentPartial) * kStaticPartials);
-constexpr size_t kOffResult = kOffVar + align256(sizeof(double) * 2 * scb::kVarChunks);
+constexpr size_t kOffWork = kOffVar + align256(sizeof(double) * 2 * scb::kVarChunks);
+constexpr size_t kOffLists = kOffWork + align256(sizeof(float) * scb::order_work_floats(kStaticMaxChannels));
+constexpr size_t kOffResult = kOffLists + align256(sizeof(int) * scb::order_list_entries(kStaticMaxChannels));
 constexpr size_t kScratchBytes =
     kOffResult + align256(sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kStaticMaxCands);
 
@@ -126,6 +129,8 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   scb::SelectState* sel = reinterpret_cast<scb::SelectState*>(b + kOffSelect);
   scb::MomentPartial* partials = reinterpret_cast<scb::MomentPartial*>(b + kOffPartials);
   double* var = reinterpret_cast<double*>(b + kOffVar);
+  float* work = reinterpret_cast<float*>(b + kOffWork);
+  int* lists = reinterpret_cast<int*>(b + kOffLists);
   scb::SearchHeader* hdr = reinterpret_cast<scb::SearchHeader*>(b + kOffResult);
   scb::Candidate* cands = reinterpret_cast<scb::Candidate*>(b + kOffResult + sizeof(scb::SearchHeader));
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
@@ -157,6 +162,8 @@ int sc_dd_search_static(const float* dev_input, long long row_stride, int num_ti
   sd.sel = sel;
   sd.partials = partials;
   sd.var = var;
+  sd.work = work;
+  sd.lists = lists;
   sd.hdr = hdr;
   sd.cands = cands;
   sd.cand_cap = kStaticMaxCands;

@@ -13,7 +13,8 @@
 //     reference's std::accumulate with a double start) the values between the two
 //     percentiles' ranges; the finaliser adds the boundary candidates and ties exactly and
 //     forms the mean with the reference's roundings (float sum, float division).
-//   * var_chunk_kernel + var_emulate_kernel: the variance.  The reference accumulates
+//   * var_chunk_kernel + var_emulate_kernel: the variance (searches whose order statistics
+//     sit on repeated values are redone exactly in the reference's order by dd_order.cu).  The reference accumulates
 //     (f - m)^2 in FLOAT, one term at a time (dedoppler.cu:257-261).  Once the
 //     accumulator is large, every term is rounded to the accumulator's ulp and terms
 //     under half an ulp vanish, which biases the sum low (about 4e-4 relative at 2^20
@@ -25,6 +26,7 @@
 //     float sum to about 1e-5 relative; the remaining difference comes from the order
 //     (the reference's order is whatever std::nth_element leaves).
 #include <algorithm>
+#include <climits>
 
 #include "dd_common.cuh"
 #include "dd_internal.h"
@@ -456,6 +458,11 @@ __global__ void __launch_bounds__(kSelThreads) select_finish_kernel(const __grid
   const float m = sum_f / (float)n;  // dedoppler.cu:255-256: float sum / count
   hdr->median = v_mid;
   hdr->mean = m;
+  // How often the most repeated of the three order-statistic values occurs: column sums with
+  // many equal values (integer-valued power) are where the order of the float variance sum
+  // matters, and those searches take the exact statistics of dd_order.cu.
+  hdr->ties = (int)min(max(s_eq[0], max(s_eq[1], s_eq[2])), (long long)INT_MAX);
+  hdr->order_exact = 0;
   st->mean = m;
   st->n = n;
   st->n_lo = n_lo;
@@ -672,7 +679,7 @@ cudaError_t column_sums_batch(const SearchBatch& b, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-cudaError_t search_stats_batch(const SearchBatch& b, int num_sms, cudaStream_t stream) {
+cudaError_t search_stats_emulated(const SearchBatch& b, int num_sms, cudaStream_t stream) {
   if (b.count <= 0) return cudaSuccess;
   const int maxN = b.maxN;
   // About four CTAs per SM over the whole batch, at least 8 per search.

@@ -189,8 +189,9 @@ def test_multibeam_band_matches_reference_gpu(torch_cuda, ref_gpu):
         cc = band * cpb + lc
         hits = []
         for b in range(3):
-            hits += ref_search(ref_gpu, host[b, :, lc * fft:(lc + 1) * fft], T, spec.foff_mhz, spec.tsamp, 3.0, 0.0,
-                               8.0, beam=b, coarse=cc)
+            # the reference context's metadata lists no beams, so its hits carry NO_BEAM: keep b
+            hits += [dict(h, beam=b) for h in ref_search(ref_gpu, host[b, :, lc * fft:(lc + 1) * fft], T,
+                                                          spec.foff_mhz, spec.tsamp, 3.0, 0.0, 8.0, beam=b, coarse=cc)]
         ctx = ref_gpu.context(T, fft, spec.foff_mhz, spec.tsamp)
         ctx.load(np.ascontiguousarray(host[3, :, lc * fft:(lc + 1) * fft]))
         inc = ctx.add_incoherent(hits)
