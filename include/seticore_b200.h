@@ -69,11 +69,10 @@ typedef struct sc_dd_stats {
   double norm_std;        /* precision form: FP64 standard deviation, used to normalise */
   int order_exact;        /* 1: median, mean and std_dev were formed in the order the
                              reference's std::nth_element calls leave the column sums, so they
-                             are bit-identical to the reference's (searches whose order
-                             statistics sit on repeated column-sum values, or every search
-                             after sc_dd_set_exact_statistics(1)); 0: median and mean exact,
-                             the float variance emulated in channel order (std_dev within
-                             about 1e-5 relative of the reference's on distinct values) */
+                             are bit-identical to the reference's (searches whose 5 %, 50 % or
+                             95 % order statistic sits on a value held by 8 or more column sums,
+                             or every search after sc_dd_set_exact_statistics(1)); 0: median and
+                             mean exact, the float variance emulated in channel order */
   int pad2;
 } sc_dd_stats;
 
@@ -162,13 +161,14 @@ const char* sc_dd_version(void);
 int sc_dd_set_stage_wait_limit(int tries);
 
 /* No counterpart in the reference (which always forms its statistics in one order).
- * mode 0 (the default): searches whose column sums put repeated values at the 5 %, 50 % or
- * 95 % order statistics -- integer-valued power, where the order of the reference's float
- * variance sum moves it by up to a few 1e-4 -- get the statistics in the reference's own
- * std::nth_element order, bit-identical; the others emulate the float sum in channel order
- * (within about 1e-5).  mode 1: every search takes the exact order (about 4 ms per batch of
- * up to 64 searches of 2^20 channels, one CTA per search).  Process-wide; launches queued
- * after the call follow it (a CUDA graph keeps the mode it was captured with). */
+ * mode 0 (the default): a search whose 5 %, 50 % or 95 % order statistic sits on a value held
+ * by 8 or more column sums -- integer-valued power, where the order of the reference's float
+ * variance sum moves the deviation by up to a few 1e-4 -- gets its statistics in the
+ * reference's own std::nth_element order, bit-identical; the others emulate the float sum in
+ * channel order (measured 2e-5 to 4e-5 relative on distinct-valued column sums, up to 3e-4
+ * on heavy-tailed ones).  mode 1: every search takes the exact order (about 4 ms per batch of
+ * 64 searches of 2^20 channels).  Process-wide; launches queued after the call follow it (a
+ * CUDA graph keeps the mode it was captured with).  Other modes: SC_DD_EINVAL. */
 int sc_dd_set_exact_statistics(int mode);
 
 /* The device half of H5Reader::loadCoarseChannel (h5_reader.cpp:190-209) for `count`
@@ -253,7 +253,7 @@ const char* sc_dd_pool_last_error(void);
  * Same inputs, results and ordering as sc_dd_search, plus the shape (unrounded
  * num_timesteps, num_channels, foff in MHz, tsamp in s) that sc_dd_create would take.
  * It calls no cudaMalloc, cudaFree, cudaMallocHost or other allocating routine: its scratch
- * is one fixed device array inside the library (about 10.1 MB, held by every GPU that loads
+ * is one fixed device array inside the library (22.8 MB, held by every GPU that loads
  * the library until the process exits) and its host side uses the stack and `out`.
  * Limits (SC_DD_ELIMIT beyond them): num_channels <= SC_DD_STATIC_MAX_CHANNELS, rounded
  * timesteps <= 16, at most 65536 windows (num_channels / window_size).  A max_drift that is

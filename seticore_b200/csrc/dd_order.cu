@@ -1317,7 +1317,7 @@ int rounds_for(long long n) {
     n = n / 2 + 1;
     ++r;
   }
-  return r + 2;
+  return r + 1;
 }
 }  // namespace
 
