@@ -46,6 +46,11 @@ class RefHit(ctypes.Structure):
                 ("frequency", ctypes.c_double)]
 
 
+class RefEventHit(ctypes.Structure):
+    _fields_ = [("present", ctypes.c_int), ("index", ctypes.c_int), ("drift_steps", ctypes.c_int),
+                ("snr", ctypes.c_float), ("power", ctypes.c_float)]
+
+
 def available(kind="port"):
     return os.path.exists(PATHS[kind])
 
@@ -140,7 +145,47 @@ class RefGpu:
         L.ref_gpu_time_search.restype = ctypes.c_double
         L.ref_gpu_add_incoherent.argtypes = [vp, ctypes.POINTER(RefHit), ctypes.c_int]
         L.ref_gpu_taylor.argtypes = [_f32, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32]
+        if hasattr(L, "ref_find_events"):
+            L.ref_find_events.argtypes = [
+                ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
+                ctypes.POINTER(ctypes.POINTER(ctypes.c_float)), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                ctypes.c_double, ctypes.c_double, ctypes.POINTER(RefEventHit), ctypes.c_int]
+            L.ref_find_events.restype = ctypes.c_int
         self.lib = L
+
+    def find_events(self, files, max_drift, snr_on, snr_off, cap=1024):
+        """The reference's findEvents (find_events.cpp:65-226) over in-memory files.
+
+        files: dicts with `rows` ([num_timesteps][num_coarse * coarse_size] float32),
+        source_name, tstart and the shared shape/metadata keys coarse_size, num_coarse, fch1,
+        foff, tsamp, has_dc_spike.  Returns the events as lists with one entry per file:
+        None or a dict of the hit's index, drift_steps, snr and power."""
+        if not hasattr(self.lib, "ref_find_events"):
+            raise OSError("libref_gpu.so predates ref_find_events: rebuild with `make -C oracle`")
+        n = len(files)
+        f0 = files[0]
+        rows = [np.ascontiguousarray(f["rows"], dtype=np.float32) for f in files]
+        names = (ctypes.c_char_p * n)(*[f["source_name"].encode() for f in files])
+        tstarts = (ctypes.c_double * n)(*[float(f["tstart"]) for f in files])
+        ptrs = (ctypes.POINTER(ctypes.c_float) * n)(
+            *[r.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) for r in rows])
+        out = (RefEventHit * (cap * n))()
+        ne = self.lib.ref_find_events(n, names, tstarts, ptrs, rows[0].shape[0], int(f0["coarse_size"]),
+                                      int(f0["num_coarse"]), float(f0["fch1"]), float(f0["foff"]),
+                                      float(f0["tsamp"]), int(bool(f0["has_dc_spike"])), float(max_drift),
+                                      float(snr_on), float(snr_off), out, cap)
+        if ne < 0:
+            raise RuntimeError("reference findEvents raised")
+        events = []
+        for e in range(min(ne, cap)):
+            ev = []
+            for k in range(n):
+                h = out[e * n + k]
+                ev.append(dict(index=h.index, drift_steps=h.drift_steps, snr=h.snr, power=h.power)
+                          if h.present else None)
+            events.append(ev)
+        return events
 
     def taylor(self, x, db):
         x = np.ascontiguousarray(x, dtype=np.float32)

@@ -228,46 +228,36 @@ scb::LevelPlan pool_level_plan(void* ctx, const scb::ExecSearch& s, float* la, f
   return best;
 }
 
-int ensure_device(sc_dd_pool* p, size_t arena, size_t lvl, size_t host) {
+// Grows the arena and the level buffers in stream order on `stream` (cudaFreeAsync /
+// cudaMallocAsync): every earlier call of this pool has finished with them (a call
+// synchronises its stream before it returns), and work of other streams -- another pool's,
+// another server worker's -- is not waited for, as a device-wide synchronisation or a plain
+// cudaFree would.  Graphs captured over the old buffers are dropped.
+int ensure_device(sc_dd_pool* p, size_t arena, size_t lvl, cudaStream_t stream) {
   cudaError_t e;
-  if (arena > p->arena_bytes) {
-    cudaDeviceSynchronize();
-    cudaFree(p->arena);
-    p->arena = nullptr;
-    p->arena_bytes = 0;
+  if (arena > p->arena_bytes || lvl > p->lvl_floats) {
     for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
     p->graphs.clear();
     p->seen.clear();
-    if ((e = cudaMalloc(&p->arena, arena)) != cudaSuccess)
+  }
+  if (arena > p->arena_bytes) {
+    if (p->arena) cudaFreeAsync(p->arena, stream);
+    p->arena = nullptr;
+    p->arena_bytes = 0;
+    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&p->arena), arena, stream)) != cudaSuccess)
       return pfail(SC_DD_ENOMEM, std::string("pool arena: ") + cudaGetErrorString(e));
-    cudaMemset(p->arena, 0, arena);
+    if ((e = cudaMemsetAsync(p->arena, 0, arena, stream)) != cudaSuccess) return pcuda(e, "pool arena memset");
     p->arena_bytes = arena;
   }
   if (lvl > p->lvl_floats) {
-    cudaDeviceSynchronize();
-    cudaFree(p->lvl_a);
+    if (p->lvl_a) cudaFreeAsync(p->lvl_a, stream);
     p->lvl_a = p->lvl_b = nullptr;
     p->lvl_floats = 0;
-    for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
-    p->graphs.clear();
-    p->seen.clear();
     // Both level buffers in one allocation: the emitting level addresses them as one array.
-    if ((e = cudaMalloc(&p->lvl_a, 2 * lvl * sizeof(float))) != cudaSuccess)
+    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&p->lvl_a), 2 * lvl * sizeof(float), stream)) != cudaSuccess)
       return pfail(SC_DD_ENOMEM, std::string("pool level buffers: ") + cudaGetErrorString(e));
     p->lvl_b = p->lvl_a + lvl;
     p->lvl_floats = lvl;
-  }
-  if (host > p->host_bytes) {
-    cudaDeviceSynchronize();
-    if (p->host) cudaFreeHost(p->host);
-    p->host = nullptr;
-    p->host_bytes = 0;
-    for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
-    p->graphs.clear();
-    p->seen.clear();
-    if ((e = cudaMallocHost(&p->host, host)) != cudaSuccess)
-      return pfail(SC_DD_ENOMEM, std::string("pool host buffer: ") + cudaGetErrorString(e));
-    p->host_bytes = host;
   }
   return SC_DD_OK;
 }
@@ -312,7 +302,12 @@ int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking);
   for (cudaEvent_t* ev : {&p->ev0, &p->ev1, &p->evj, &p->t0, &p->t1})
     if (e == cudaSuccess) e = cudaEventCreate(ev);
+  // The host buffer of the largest possible sub-batch, allocated once: pinned allocations
+  // synchronise the device, which a pool serving beside other streams must not do per call.
+  p->host_bytes = (size_t)4 * scb::kMaxBatch * (sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands);
+  if (e == cudaSuccess) e = cudaMallocHost(&p->host, p->host_bytes);
   if (e != cudaSuccess) {
+    if (p->host) cudaFreeHost(p->host);
     delete p;
     return pcuda(e, "sc_dd_pool_create");
   }
@@ -326,8 +321,9 @@ int sc_dd_pool_destroy(sc_dd_pool* p) {
   if (!p) return SC_DD_OK;
   cudaDeviceSynchronize();
   for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
-  cudaFree(p->arena);
-  cudaFree(p->lvl_a);
+  if (p->arena) cudaFreeAsync(p->arena, nullptr);
+  if (p->lvl_a) cudaFreeAsync(p->lvl_a, nullptr);
+  cudaDeviceSynchronize();
   if (p->host) cudaFreeHost(p->host);
   for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1})
     if (ev) cudaEventDestroy(ev);
@@ -425,11 +421,7 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
     for (const Planned& pl : plans)
       if (pl.es.Tr > 32) lvl_need = std::max(lvl_need, scb::level_buffer_floats(pl.es.Tr, pl.es.N));
   }
-  size_t host_need = 0;
-  for (auto& sb : subs)
-    host_need = std::max(host_need, (size_t)(sb.second - sb.first) *
-                                        (sizeof(scb::SearchHeader) + sizeof(scb::Candidate) * kHostCands));
-  int rc = ensure_device(p, arena_need, lvl_need, host_need);
+  int rc = ensure_device(p, arena_need, lvl_need, stream);
   if (rc != SC_DD_OK) return rc;
 
   cudaError_t e;

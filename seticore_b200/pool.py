@@ -53,7 +53,12 @@ class SearchPool:
     def __init__(self, scratch_budget_bytes: int = 8 << 30, autotune: bool = True, cuda_graphs: bool = True):
         self._h = ctypes.c_void_p()
         check(lib().sc_dd_pool_create(scratch_budget_bytes, ctypes.byref(self._h)), pool=True)
-        check(lib().sc_dd_pool_configure(self._h, int(autotune), int(cuda_graphs)), pool=True)
+        self._graphs = bool(cuda_graphs)
+        self.configure(autotune)
+
+    def configure(self, autotune: bool):
+        """Turns the timing of new launch classes on or off (tuned classes stay tuned)."""
+        check(lib().sc_dd_pool_configure(self._h, int(autotune), int(self._graphs)), pool=True)
 
     def close(self):
         if self._h:

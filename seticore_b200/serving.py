@@ -58,6 +58,8 @@ class SearchServer:
         self.stats = {"batches": 0, "requests": 0, "max_inflight_bytes": 0, "overlapped_batches": 0}
         self._running = 0
         self._threads = []
+        self._pools = []
+        self._autotune = True
         for i in range(workers):
             t = threading.Thread(target=self._work, args=(torch.cuda.Stream(),), daemon=True, name=f"dd-serve-{i}")
             t.start()
@@ -81,6 +83,15 @@ class SearchServer:
         for t in self._threads:
             t.join()
 
+    def set_autotune(self, enabled: bool):
+        """Tuning times each new launch class on first sight, with synchronisations that stall
+        a worker: a server warmed on its traffic turns it off, and classes not seen during the
+        warm-up then take the default launch shape."""
+        with self._cv:
+            self._autotune = bool(enabled)
+            for p in self._pools:
+                p.configure(self._autotune)
+
     def _take(self) -> List[_Pending]:
         """Pending requests, in arrival order, that fit the free budget (at most max_batch)."""
         n = admit([p.bytes for p in self._q], self.budget - self.used, self.max_batch)
@@ -91,6 +102,9 @@ class SearchServer:
         # Arrival-time batches rarely repeat a composition, so captured graphs would seldom
         # replay; launch shapes are still tuned per shape class on first sight.
         pool = SearchPool(scratch_budget_bytes=max(1 << 30, self.budget // 8), cuda_graphs=False)
+        with self._cv:
+            pool.configure(self._autotune)
+            self._pools.append(pool)
         while True:
             with self._cv:
                 while not self._stop and not (self._q and self._q[0].bytes <= self.budget - self.used):

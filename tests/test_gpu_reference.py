@@ -203,3 +203,71 @@ def test_multibeam_band_matches_reference_gpu(torch_cuda, ref_gpu):
             for h in got]
     assert sorted(mine) == sorted(want)
     assert len(want) >= 6
+
+
+def _cadence(T, N, num_coarse, seed):
+    """Six ABACAD files of num_coarse coarse channels with drifting tones placed so that some
+    become events and some do not (in every file; zero drift; a matching hit in an "off")."""
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    # channels per timestep: a whole number of drift steps over the rounded rows, slow enough
+    # with padding rows that expectedIndex (drift over num_timesteps - 1) stays in the wiggle
+    rate = 8.0 / 15.0 if T == 16 else 0.25
+    files = []
+    for i in range(6):
+        parts = []
+        for cc in range(num_coarse):
+            spec = SearchSpec(T, N, seed=seed + 10 * i + cc, n_tones=0)
+            parts.append(make_filterbank_numpy(spec)[:T])
+        x = np.concatenate(parts, axis=1)
+        sigma = np.std(np.sort(parts[0].sum(axis=0, dtype=np.float64))[int(np.ceil(0.05 * N)):int(0.95 * N) + 1])
+        tstart = i * 300.0
+        t_off = tstart / spec.tsamp
+        on = i % 2 == 0
+
+        def tone(cc, c0, r, snr):
+            for t in range(T):
+                c = c0 + int(round(r * t_off)) + int(round(t * r))
+                if 0 <= c < N:
+                    x[t, cc * N + c] += snr * sigma / T
+
+        tone(0, N // 8, rate, 40)                   # in every file: no event
+        if on:
+            tone(0, 5 * N // 8, rate, 40)           # ons only: an event
+            tone(0, 3 * N // 8, rate, 40)           # ons, and an off below: no event
+        if i == 3:
+            tone(0, 3 * N // 8, rate, 18)
+        if num_coarse > 1 and on:
+            tone(1, N // 4, 0.0, 60)                # zero drift: removed
+            tone(1, 3 * N // 4, -rate, 35)          # negative drift: an event
+        files.append(dict(rows=x, source_name="TGT" if on else f"OFF{i}", tstart=tstart, coarse_size=N,
+                          num_coarse=num_coarse, fch1=8000.0, foff=spec.foff_mhz, tsamp=spec.tsamp,
+                          has_dc_spike=True))
+    return files
+
+
+@pytest.mark.parametrize("T,num_coarse", [(16, 2), (12, 1)])
+def test_find_events_match_reference_gpu(torch_cuda, ref_gpu, tmp_path, T, num_coarse):
+    """Cadence search (find_events.cpp:65-226) against the reference's own findEvents built
+    with its Dedopplerer: the same events, each file's hit with the same index and drift,
+    power bit-equal and SNR within 1e-4 relative (None in the same files)."""
+    from seticore_b200.events import findEvents
+    from seticore_b200.run_dedoppler import ArrayFilterbankFile
+    N = 1 << 15
+    files = _cadence(T, N, num_coarse, 7000 + T)
+    max_drift, snr_on, snr_off = 2.0, 20.0, 14.0
+    want = ref_gpu.find_events(files, max_drift, snr_on, snr_off)
+    readers = [ArrayFilterbankFile(f["rows"], coarse_channel_size=N, telescope_id=6, foff=f["foff"],
+                                   tsamp=f["tsamp"], tstart=f["tstart"], fch1=f["fch1"],
+                                   source_name=f["source_name"]) for f in files]
+    assert all(r.has_dc_spike for r in readers)
+    got = findEvents(readers, str(tmp_path / "c.events"), max_drift, snr_on, snr_off, verbose=False)
+    assert len(want) >= 1, want
+    assert len(got) == len(want), (got, want)
+    for ev_got, ev_want in zip(got, want):
+        assert [h is None for h in ev_got] == [h is None for h in ev_want]
+        for g, w in zip(ev_got, ev_want):
+            if w is None:
+                continue
+            assert (g.index, g.drift_steps) == (w["index"], w["drift_steps"])
+            assert np.float32(g.power) == np.float32(w["power"])
+            assert abs(g.snr - w["snr"]) <= 1e-4 * abs(w["snr"])
