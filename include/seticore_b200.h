@@ -160,6 +160,15 @@ const char* sc_dd_version(void);
  * without a fault.  Process-wide; a CUDA graph keeps the limit it was captured with. */
 int sc_dd_set_stage_wait_limit(int tries);
 
+/* Tuning and test hook, no counterpart in the reference.  A search of 64 to 256 rounded
+ * timesteps runs its first (16-row) level and its last level in stripe passes: each pass
+ * writes the planes of a range of channels and a few drift blocks.  bytes > 0 bounds the
+ * planes of one pass (narrower passes, which keep their planes in L2 with eviction hints);
+ * 0 lets a pass cover whole rows; bytes < 0 restores the default (whole rows, or
+ * SETICORE_B200_LEVEL_L2_MB).  Results do not depend on it.  Process-wide; a CUDA graph
+ * keeps the passes it was captured with. */
+int sc_dd_set_level_stripe_bytes(long long bytes);
+
 /* No counterpart in the reference (which always forms its statistics in one order).
  * mode 0 (the default): a search whose 5 %, 50 % or 95 % order statistic sits on a value held
  * by 8 or more column sums -- integer-valued power, where the order of the reference's float

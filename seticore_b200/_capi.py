@@ -33,6 +33,7 @@ EXPORTED = [
     "sc_dd_pool_create", "sc_dd_pool_destroy", "sc_dd_pool_configure", "sc_dd_pool_search",
     "sc_dd_pool_stats_get", "sc_dd_request_scratch_bytes", "sc_dd_pool_last_error",
     "sc_dd_prepare_coarse_channels", "sc_dd_gather_columns", "sc_dd_set_stage_wait_limit",
+    "sc_dd_set_level_stripe_bytes",
     "sc_dd_set_exact_statistics",
 ]
 
@@ -149,6 +150,7 @@ def lib():
         L.sc_dd_prepare_coarse_channels.argtypes = [vp, i, ll, ll, i, i, i, i, vp]
         L.sc_dd_gather_columns.argtypes = [vp, ll, i, i, vp, vp, i, vp, vp]
         L.sc_dd_set_stage_wait_limit.argtypes = [i]
+        L.sc_dd_set_level_stripe_bytes.argtypes = [ctypes.c_longlong]
         L.sc_dd_set_exact_statistics.argtypes = [i]
         L.sc_dd_last_error.restype = ctypes.c_char_p
         L.sc_dd_version.restype = ctypes.c_char_p

@@ -447,6 +447,11 @@ int sc_dd_set_stage_wait_limit(int tries) {
   return SC_DD_OK;
 }
 
+int sc_dd_set_level_stripe_bytes(long long bytes) {
+  scb::set_level_stripe_bytes(bytes);
+  return SC_DD_OK;
+}
+
 int sc_dd_set_exact_statistics(int mode) {
   if (mode != 0 && mode != 1) return fail(SC_DD_EINVAL, "sc_dd_set_exact_statistics: mode must be 0 or 1");
   scb::set_exact_statistics_always(mode == 1);

@@ -54,6 +54,32 @@ __device__ __forceinline__ float path_sum_pairwise(int L, int off, Get get) {
   return stack[0];
 }
 
+// The same sum for L = 2^n rows with the channel offset advanced incrementally: going from
+// row t to t + 1 clears the trailing one bits of t (the blocks whose second halves end
+// there, which the pairwise merges close in the same loop) and sets the next bit, so the
+// offset drops the shifts of the cleared levels and gains the shift of the set one
+// (level m shifts a block's second half by ((off >> (n-1-m)) + 1) >> 1).  Bit-identical to
+// path_sum_pairwise; about two loop steps per row instead of n.
+template <typename Get>
+__device__ __forceinline__ float path_sum_pow2(int n, int off, Get get) {
+  float stack[12];
+  int depth = 0, p = 0;
+  const int L = 1 << n;
+  for (int t = 0; t < L; ++t) {
+    float v = get(t, p);
+    int k = t, m = 0, sub = 0;
+    while (k & 1) {
+      v = stack[--depth] + v;
+      sub += ((off >> (n - 1 - m)) + 1) >> 1;
+      k >>= 1;
+      ++m;
+    }
+    stack[depth++] = v;
+    if (m < n) p += (((off >> (n - 1 - m)) + 1) >> 1) - sub;
+  }
+  return stack[0];
+}
+
 // Float -> unsigned key with the same order as the float values (non-NaN).
 __device__ __forceinline__ uint32_t float_key(float f) {
   const uint32_t u = __float_as_uint(f);

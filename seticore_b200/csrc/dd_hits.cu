@@ -80,6 +80,7 @@ __global__ void resolve_kernel(const __grid_constant__ SearchBatch b) {
   const long long n = min(hdr->num_candidates, cap);
   const long long npaths = (long long)(dmax - dmin + 1) * Tr;
   const long long total = n * npaths;
+  const int levels = 31 - __clz(Tr);  // Tr is a power of two
   for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     const long long i = idx / npaths;
@@ -89,7 +90,7 @@ __global__ void resolve_kernel(const __grid_constant__ SearchBatch b) {
     const int off = p - (p / Tr) * Tr;
     const long long e = (long long)(Tr - 1) * db;
     if (c + e < 0 || c + e + off >= N) continue;
-    const float v = path_sum_pairwise(Tr, off, [&](int t, int pos) {
+    const float v = path_sum_pow2(levels, off, [&](int t, int pos) {
       return __ldg(in + (long long)t * stride + c + (long long)db * t + pos);
     });
     if (v > 0.0f) {  // the reference's top sums start at zero and update on strict >

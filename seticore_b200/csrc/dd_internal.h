@@ -143,9 +143,15 @@ struct TreeGroup {
   float* emit_out;
   long long emit_job_stride;
   long long emit_plane_stride;
+  // Optional channel range of the group's tiles: the tiles that cover [x_begin, x_end), with
+  // x_begin a multiple of the launch's tile width (x_end == 0: every tile of [0, N); x_end < 0:
+  // none).
+  int x_begin;
+  int x_end;
   int jobs_per_chunk;
   int n_chunks;
   int n_tiles;
+  int tile_first;
   int item_begin;  // first work item of this group in the launch
   // Optional: set to 1 if a staging wait of the tree gave up (its results are then invalid).
   int* status;
@@ -157,6 +163,9 @@ struct TreeBatch {
   // Polls of the staging wait before a CTA gives up (negative: the default, about a second).
   // The launcher fills it from stage_wait_tries().
   int stage_wait_tries = -1;
+  // L2 hints of the bulk copies: 0 none; 1 (stripe passes' first level) staged input rows
+  // evict-first and emitted planes evict-last, so the planes stay in L2 for the last level.
+  int cache_mode = 0;
   TreeGroup g[kMaxBatch];
 };
 
@@ -183,8 +192,10 @@ cudaError_t tree_max_batch(TreeBatch& b, int R, int num_sms, cudaStream_t stream
 // The same staged tree for 16 rows, writing every root value (all 16 in-block offsets of
 // every channel) to the groups' emit planes instead of folding maxima: the first level of
 // a tree of more than 32 rows.  Values of paths that leave [0, N) are sums with zeros.
-// Every tile is stored whole, so plane rows must hold level_row_length(N) floats.
-cudaError_t tree_emit_batch(TreeBatch& b, int num_sms, cudaStream_t stream, int smem_budget_kb = 0);
+// Every 352-channel tile is stored whole, so plane rows must hold level_row_length(N)
+// floats.  nparts: the offsets in two halves of eight (2) or all sixteen in one warp (1).
+// Float rows only.
+cudaError_t tree_emit_batch(TreeBatch& b, int num_sms, cudaStream_t stream, int smem_budget_kb = 0, int nparts = 2);
 
 // Channels per tree work item (the tile a flag refers to).
 int tree_tile_width();
@@ -196,7 +207,13 @@ inline long long level_row_length(int N) {
   const long long w = tree_tile_width();
   return (N + w - 1) / w * w;
 }
-inline size_t level_buffer_floats(int Tr, int N) { return (size_t)Tr * (size_t)level_row_length(N); }
+// The slack of each row covers the stripe passes' per-row channel origins and shears
+// (one drift block of a last level of up to 16 rows, dd_levels.cu), so a whole row always
+// fits one pass.
+constexpr long long kLevelRowSlack = 1408;
+inline size_t level_buffer_floats(int Tr, int N) {
+  return (size_t)Tr * (size_t)(level_row_length(N) + kLevelRowSlack);
+}
 
 // Precision form (dd_precision.cu), per search of a batch:
 struct PrecisionDesc {
@@ -286,11 +303,15 @@ cudaError_t path_values(const float* input, long long row_stride, int Tr, int N,
 // kStreamEmit16 (the emitting form of the fused tree) -- then a fused max level of
 // final_rows (2, 4, 8 or 16) rows.  n == 0: the default split.
 constexpr int kStreamEmit16 = 1016;
+constexpr int kStreamEmit16One = 1017;  // the emitting form with all sixteen offsets in one warp
 struct LevelPlan {
   int n;
   int m[12];
   int final_rows;
 };
+
+// L2 budget of one stripe pass of the one-level split (bytes; negative: the default).
+void set_level_stripe_bytes(long long bytes);
 
 // Multi-level tree for Tr > 32 (one search): level kernels write the partial planes of
 // every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).

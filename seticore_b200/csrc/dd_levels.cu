@@ -20,6 +20,8 @@
 // pairing of the adds is the tree's own at every level, so every path sum is
 // bit-identical to the reference's twoStageTaylorTree (taylor.cu:298-327).
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -170,9 +172,10 @@ TreeGroup final_group(const float* src, long long Np, int N, int final_rows, int
   return tp;
 }
 
-// The emitting 16-row tree for drift blocks db0 .. db0 + nj - 1 of the input's Tr rows:
-// group q reads rows 16q .. 16q + 15 (one trapezoid for the nj drift blocks) and writes
-// plane r*(Tr/16) + q of drift block j to out + j*job_stride.
+// The emitting 16-row tree for drift blocks db0 .. db0 + nj - 1 of the input's Tr rows
+// (whole rows, the plane layout of the other level kernels): group q reads rows
+// 16q .. 16q + 15 (one trapezoid for the nj drift blocks) and writes plane r*(Tr/16) + q of
+// drift block j to out + j*job_stride.
 cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long long Np, int db0, int nj,
                    float* out, long long job_stride, int num_sms, cudaStream_t stream, int* status) {
   const int nb = Tr / 16;
@@ -197,7 +200,191 @@ cudaError_t emit16(const float* input, long long row_stride, int Tr, int N, long
   return tree_emit_batch(eb, num_sms, stream);
 }
 
+constexpr int kEmitTile = 352;     // channels per work item of the emitting tree
+constexpr int kStripeUnit = 5280;  // stripes start at multiples of every tree tile width (160, 352, 1056)
+
+// Bytes of planes one stripe pass may write: set_level_stripe_bytes, else
+// SETICORE_B200_LEVEL_L2_MB, else 0, which keeps whole rows (as many drift blocks per pass
+// as the level buffers hold).  Passes narrower than the row mark their input reads
+// evict-first and their planes evict-last in L2, but on 64 x 256 x 131072 beams budgets of
+// 32 to 96 MB still measured 0.6-0.95x the whole-row passes: the last level's reads did not
+// come from L2, and the narrow passes leave each launch too few items per CTA.
+std::atomic<long long> g_stripe_bytes{-1};
+size_t level_l2_bytes() {
+  const long long set = g_stripe_bytes.load();
+  if (set >= 0) return (size_t)set;
+  static const size_t mb = [] {
+    const char* e = getenv("SETICORE_B200_LEVEL_L2_MB");
+    const long v = e ? strtol(e, nullptr, 10) : -1;
+    return (v >= 0 && v <= 4096) ? (size_t)v : (size_t)0;
+  }();
+  return mb << 20;
+}
+
+// L2 hints in stripe passes (SETICORE_B200_LEVEL_HINTS=0 turns them off, for comparisons).
+bool level_cache_hints() {
+  static const bool on = [] {
+    const char* e = getenv("SETICORE_B200_LEVEL_HINTS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Drift blocks per stripe pass at most (SETICORE_B200_LEVEL_MAXJ, for tuning; default 64).
+int level_max_chunk() {
+  static const int v = [] {
+    const char* e = getenv("SETICORE_B200_LEVEL_MAXJ");
+    const long x = e ? strtol(e, nullptr, 10) : 0;
+    return (x >= 1 && x <= kMaxBatch) ? (int)x : kMaxBatch;
+  }();
+  return v;
+}
+
+// Row length of a stripe pass's planes: a stripe of L channels, nj drift blocks, a last
+// level of fr rows.  Block row q of the planes starts at channel x_b - 704 + 16*d0*q (its
+// own origin, so a row holds only the channels that the last level reads in that row):
+// the stripe, the shears of the nj drift blocks' sixteen sub-problems over q <= fr - 1
+// rows, the last tile's lead and the rounding of both tile widths.
+long long stripe_row_length(long long L, int nj, int fr) {
+  return (L + (16ll * nj - 1) * (fr - 1) + fr + 1062 + 3) / 4 * 4;
+}
+
+// One stripe pass of a one-level split (Tr = 16 * fr rows, fr <= 16): the emitting 16-row
+// tree writes, for drift blocks d0 .. d0 + nj - 1, the planes that the last level reads for
+// the output tiles of [x_b, x_e), then the last level folds them into top.  plane(r, q) of
+// drift block j at channel c is G[j*Tr*Lp + r*fr*Lp + q*(Lp - 16*d0) + c], with
+// G = buf + 704 - x_b (each block row has its own channel origin).  A pass's planes fit the
+// L2 budget, so the last level reads them from L2 and the next pass rewrites the same lines.
+cudaError_t stripe_pass(const float* input, long long row_stride, int Tr, int N, int d0, int nj,
+                        long long x_b, long long x_e, long long Lp, float* buf, float* top, int nparts, int num_sms,
+                        cudaStream_t stream, int* status) {
+  const int fr = Tr / 16;
+  const long long etile = kEmitTile;
+  float* G = buf + 704 - x_b;
+  const long long qstride = Lp - 16ll * d0;
+  // The last level's tiles: 352 channels, 1056 for last levels of 4 rows or fewer
+  // (tree_max_batch's choice for jobs with their own rows).
+  const long long WF = fr <= 4 ? 1056 : kEmitTile;
+  const long long x_tiles_end = (x_e + WF - 1) / WF * WF;
+  TreeBatch eb;
+  eb.count = fr;
+  eb.n_items = 0;
+  eb.cache_mode = level_cache_hints() && (x_b > 0 || x_e < N) ? 1 : 0;  // stripes narrower than the row
+  for (int q = 0; q < fr; ++q) {
+    TreeGroup& g = eb.g[q];
+    g = TreeGroup{};
+    g.rows = input + (long long)16 * q * row_stride;
+    g.row_stride = row_stride;
+    g.job_row_stride = 0;
+    g.N = N;
+    g.d_first = d0;
+    g.d_step = 1;
+    g.n_jobs = nj;
+    g.emit_out = G + q * qstride;
+    g.emit_job_stride = (long long)Tr * Lp;
+    g.emit_plane_stride = (long long)fr * Lp;
+    // Channels the last level reads in block row q: shears 16*(d0 + j) + k per row for
+    // k < 16, j < nj; staged windows rounded out to 16-byte chunks.
+    const long long lo = x_b + 16ll * d0 * q - 3;
+    const long long hi = x_tiles_end + (16ll * (d0 + nj - 1) + 15) * q + fr + 7;
+    const long long xb = std::max<long long>(0, lo >= 0 ? lo / etile * etile : 0);
+    const long long xe = std::min<long long>(N, hi);
+    // Every tile the level writes (and so every channel the last level reads) lies inside
+    // block row q's part of the buffer, [origin, origin + Lp).
+    const long long origin = x_b - 704 + 16ll * d0 * q;
+    const long long wend = (xe + etile - 1) / etile * etile;
+    if (xe > xb && (xb < origin || wend > origin + Lp)) return cudaErrorInvalidValue;
+    g.x_begin = (int)xb;
+    g.x_end = xe > xb ? (int)xe : -1;  // no tiles when the last level reads none of [0, N) here
+    g.status = status;
+  }
+  cudaError_t err = tree_emit_batch(eb, num_sms, stream, 0, nparts);
+  if (err != cudaSuccess) return err;
+  TreeBatch tb;
+  tb.count = nj;
+  tb.n_items = 0;
+  for (int j = 0; j < nj; ++j) {
+    TreeGroup& tp = tb.g[j];
+    tp = TreeGroup{};
+    tp.rows = G + (long long)j * Tr * Lp;
+    tp.row_stride = qstride;
+    tp.job_row_stride = (long long)fr * Lp;
+    tp.N = N;
+    tp.d_first = 16 * (d0 + j);
+    tp.d_step = 1;
+    tp.n_jobs = 16;
+    tp.db_first = d0 + j;
+    tp.db_step = 0;
+    tp.off_base = 0;
+    tp.off_step = fr;
+    tp.elig_T1 = Tr - 1;
+    tp.top = top;
+    tp.x_begin = (int)x_b;
+    tp.x_end = (int)x_e;
+    tp.status = status;
+  }
+  return tree_max_batch(tb, fr, num_sms, stream);
+}
+
+// The one-level split with the emitting first level, in stripe passes.  The planes of a
+// pass (nj drift blocks x Tr rows x the stripe) fit the L2 budget where one is set, else
+// the level buffers (`cap` floats).
+cudaError_t stripes_search(const float* input, long long row_stride, int Tr, int N, int dmin, int dmax,
+                           float* buf, long long cap, float* top, int nparts, int num_sms, cudaStream_t stream,
+                           int* status) {
+  const int fr = Tr / 16;
+  const int ndb = dmax - dmin + 1;
+  // The whole row as one stripe (x_b = 0 suits every tile width, so any tile multiple will do).
+  const long long Nt = ((long long)N + 1055) / 1056 * 1056;
+  const long long l2 = (long long)(level_l2_bytes() / sizeof(float));
+  const long long budget = l2 > 0 ? std::min(l2, cap) : cap;
+  int J = std::min(ndb, std::min(kMaxBatch, level_max_chunk()));
+  long long L = 0;
+  for (;; J = (J + 1) / 2) {
+    const long long avail = budget / ((long long)J * Tr) - stripe_row_length(0, J, fr);
+    if (avail >= Nt) {
+      L = Nt;
+      break;
+    }
+    // at least four stripe units per pass unless one drift block is left
+    L = std::max<long long>(0, avail) / kStripeUnit * kStripeUnit;
+    if (L >= 4 * kStripeUnit || J == 1) break;
+  }
+  if (L < Nt) L = std::min<long long>(std::max<long long>(L, kStripeUnit), Nt);
+  long long Lp = stripe_row_length(L, J, fr);
+  if ((long long)J * Tr * Lp > cap) {  // the smallest stripe is too long for the buffers: whole rows
+    J = 1;
+    L = Nt;
+    Lp = stripe_row_length(L, J, fr);
+    if ((long long)Tr * Lp > cap) return cudaErrorInvalidValue;  // level buffers too small
+  }
+  cudaError_t err;
+  for (int d0 = dmin; d0 <= dmax; d0 += J) {
+    const int nj = std::min(J, dmax - d0 + 1);
+    for (long long x_b = 0; x_b < N; x_b += L) {
+      const long long x_e = std::min<long long>(N, x_b + L);
+      if ((err = stripe_pass(input, row_stride, Tr, N, d0, nj, x_b, x_e, Lp, buf, top, nparts, num_sms, stream,
+                             status)) != cudaSuccess)
+        return err;
+    }
+  }
+  return cudaGetLastError();
+}
+
+// First level of the default one-level split (SETICORE_B200_LEVEL_FIRST overrides it for
+// tuning: 16, 1016 or 1017).
+int default_first_level() {
+  static const int v = [] {
+    const char* e = getenv("SETICORE_B200_LEVEL_FIRST");
+    const long x = e ? strtol(e, nullptr, 10) : 0;
+    return (x == 16 || x == kStreamEmit16 || x == kStreamEmit16One) ? (int)x : kStreamEmit16;
+  }();
+  return v;
+}
+
 }  // namespace
+
+void set_level_stripe_bytes(long long bytes) { g_stripe_bytes.store(bytes < 0 ? -1 : bytes); }
 
 cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
@@ -211,17 +398,21 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
     int prod = plan.final_rows;
     for (int l = 0; l < plan.n; ++l) {
       const int M = plan.m[l];
-      if (M != 2 && M != 4 && M != 8 && M != 16 && !(M == kStreamEmit16 && l == 0)) return cudaErrorInvalidValue;
+      const bool emit = (M == kStreamEmit16 || M == kStreamEmit16One) && l == 0;
+      if (M != 2 && M != 4 && M != 8 && M != 16 && !emit) return cudaErrorInvalidValue;
       sizes[nlev++] = M;
-      prod *= (M == kStreamEmit16) ? 16 : M;
+      prod *= emit ? 16 : M;
     }
     final_rows = plan.final_rows;
     if (prod != Tr || (final_rows != 2 && final_rows != 4 && final_rows != 8 && final_rows != 16))
       return cudaErrorInvalidValue;
   } else {
-    // Default: the one-thread-per-channel 16-row level, then 4s and 2s down to at most 16.
+    // Default: the 16-row level, then 4s and 2s down to at most 16 rows.  A single 16-row
+    // level (Tr <= 256) of float rows takes the emitting tree in stripe passes; 16-bit rows
+    // and deeper splits the four-channels-per-thread level kernel (the emitting tree
+    // converts 16-bit rows with per-thread loads as it stages them: 0.79x on 256-row beams).
     int tp = Tr / 16;
-    sizes[nlev++] = 16;
+    sizes[nlev++] = (tp <= 16 && elem == kElemF32) ? default_first_level() : 16;
     while (tp > 16) {
       const int M = (tp / 4 >= 16) ? 4 : 2;
       sizes[nlev++] = M;
@@ -236,6 +427,9 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
   const long long Np = level_row_length(N);  // plane row length
   const long long per_db = (long long)Tr * Np;
   cudaError_t err;
+  if (nlev == 1 && (sizes[0] == kStreamEmit16 || sizes[0] == kStreamEmit16One))  // float rows (checked above)
+    return stripes_search(input, row_stride, Tr, N, dmin, dmax, scratch_a, 2 * half, top,
+                          sizes[0] == kStreamEmit16One ? 1 : 2, num_sms, stream, status);
   if (nlev == 1 && (sizes[0] == 16 || sizes[0] == kStreamEmit16)) {
     // One level, then the last: the planes of up to J drift blocks per pair of launches.
     long long J = 2 * half / per_db;
@@ -244,10 +438,7 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
     const int nb = Tr / 16;
     for (int db = dmin; db <= dmax; db += (int)J) {
       const int nj = (int)std::min<long long>(J, dmax - db + 1);
-      if (sizes[0] == kStreamEmit16) {
-        if ((err = emit16(input, row_stride, Tr, N, Np, db, nj, scratch_a, per_db, num_sms, stream, status)) != cudaSuccess)
-          return err;
-      } else {
+      {
         dim3 grid((N + 511) / 512, (unsigned)(nj * nb));
         if (elem == kElemBF16)
           direct16x4_kernel<<<grid, 128, 0, stream>>>(static_cast<const __nv_bfloat16*>(input_v), row_stride, 0, Tr, db,
@@ -279,7 +470,7 @@ cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int
     for (int l = 0; l < nlev; ++l) {
       int M = sizes[l];
       const int D0 = (int)(dscale * db);
-      if (M == kStreamEmit16) {
+      if (M == kStreamEmit16 || M == kStreamEmit16One) {
         M = 16;
         if ((err = emit16(src, stride, Tp, N, Np, db, 1, dst, per_db, num_sms, stream, status)) != cudaSuccess) return err;
       } else if (M == 16) {

@@ -247,8 +247,9 @@ LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 1, 11, 3, 12),
 
 
 # (R, offset parts, U, iterations) of the emitting form: every root value goes to a sink
-# (the level kernels' output planes) instead of a running maximum.
-EMIT_CONFIGS = [(16, 2, 11, 3)]
+# (the level kernels' output planes, through a per-warp shared-memory buffer) instead of a
+# running maximum.  Short strips (S = 11) keep a warp's buffer of one tile small.
+EMIT_CONFIGS = [(16, 2, 11, 1), (16, 1, 11, 1)]
 # Subtree sizes of the one-thread-per-channel level kernel (dd_levels.cu).
 DIRECT_SIZES = [2, 4, 8, 16]
 # (rows, consecutive channels per thread) of the level kernel's multi-channel form.
