@@ -318,11 +318,16 @@ def serve_result(world, rank, local, n_inputs, serve_seconds):
         for f in [server.submit(base[i % n_inputs]) for i in range(n_cap)]:
             f.result()
         server.set_autotune(False)
-        t0 = time.perf_counter()
-        futs = [server.submit(base[i % n_inputs]) for i in range(n_cap)]
-        for f in futs:
-            f.result()
-        cap_s = time.perf_counter() - t0
+        # capacity: the median of three saturated runs, so that a one-off stall (a pool
+        # growing its arena, a first launch) does not set the offered loads
+        cap_runs = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            futs = [server.submit(base[i % n_inputs]) for i in range(n_cap)]
+            for f in futs:
+                f.result()
+            cap_runs.append(time.perf_counter() - t0)
+        cap_s = float(np.median(cap_runs))
         cap_rps = n_cap / cap_s
         samples = sum(base[i % n_inputs].input.shape[0] * base[i % n_inputs].input.shape[1] for i in range(n_cap))
         points = []
@@ -336,6 +341,7 @@ def serve_result(world, rank, local, n_inputs, serve_seconds):
         st = dict(server.stats)
         server.close()
         out["forms"][form] = {"capacity_requests_per_s": cap_rps, "capacity_gsamples_per_s": samples / cap_s / 1e9,
+                              "capacity_runs_s": cap_runs,
                               "hits_identical_to_fp32": identical, "points": points, "server": st}
     del reqs
     return out

@@ -114,7 +114,7 @@ __global__ void path_values_kernel(const float* __restrict__ in, long long strid
     out[i] = __int_as_float(0x7fc00000);
     return;
   }
-  out[i] = path_sum_pairwise(Tr, off, [&](int t, int pos) {
+  out[i] = path_sum_pow2(31 - __clz(Tr), off, [&](int t, int pos) {  // Tr is a power of two
     return __ldg(in + (long long)t * stride + c + (long long)db * t + pos);
   });
 }

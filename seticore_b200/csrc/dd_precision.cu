@@ -243,6 +243,7 @@ __global__ void recompute_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
   const long long n = *d.flag_count;
   const int Tr = d.Tr, N = d.N;
+  const int levels = 31 - __clz(Tr);  // Tr is a power of two
   const int paths = (d.dmax - d.dmin + 1) * Tr;
   const int nblk = (paths + blockDim.x - 1) / blockDim.x;
   for (long long u = blockIdx.x; u < n * nblk; u += gridDim.x) {
@@ -256,7 +257,7 @@ __global__ void recompute_kernel(const __grid_constant__ PrecisionBatch b) {
       const long long e = (long long)(Tr - 1) * db;
       if (c + e >= 0 && c + e + off < N) {  // findTopPathSums' early return (dedoppler.cu:40-46)
         const float* base = d.input + c;
-        best = fmaxf(0.0f, path_sum_pairwise(Tr, off, [&](int t, int pos) {
+        best = fmaxf(0.0f, path_sum_pow2(levels, off, [&](int t, int pos) {
           return __ldg(base + (long long)t * d.row_stride + (long long)db * t + pos);
         }));
       }
