@@ -79,8 +79,10 @@ typedef struct sc_dd_stats {
 /* Storage of the spectra the tree reads.  FP32: the input as given (the reference's
  * form).  BF16 / FP16: each search first normalises its input per coarse channel,
  * (x - mean) / std with FP64 mean and std, into a 16-bit copy; the tree accumulates in
- * FP32 over that copy, every channel whose top reaches 0.9 x the threshold is then
- * recomputed in FP32 from the original power, and the hit list equals the FP32 form's. */
+ * FP32 over that copy, every channel whose top could reach the threshold (its 16-bit top
+ * reaches the threshold less a bound on the rounding of the 16-bit values and of the FP32
+ * sums) is then recomputed in FP32 from the original power, and the hit list equals the
+ * FP32 form's. */
 enum { SC_DD_PRECISION_FP32 = 0, SC_DD_PRECISION_BF16 = 1, SC_DD_PRECISION_FP16 = 2 };
 
 typedef struct sc_dd sc_dd;
@@ -133,8 +135,9 @@ int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_
 
 /* Selects the storage form of later searches (SC_DD_PRECISION_*).  The 16-bit forms store
  * the FP64-normalised power as BF16 or FP16, sum it in FP32, and recompute in FP32, from
- * the original power, the top of every channel within 0.9 x the threshold, so their hit
- * lists equal the FP32 form's.  They allocate their scratch on first use. */
+ * the original power, the top of every channel that the rounding bound cannot exclude
+ * from the threshold, so their hit lists equal the FP32 form's.  They allocate their
+ * scratch on first use. */
 int sc_dd_set_precision(sc_dd* dd, int precision);
 
 /* Statistics of the first search of the engine's last completed call; tree_ms and

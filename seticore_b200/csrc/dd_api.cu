@@ -118,7 +118,7 @@ struct sc_dd {
   float* top16 = nullptr;        // [slot][N]
   int* flags = nullptr;          // [slot][N] flagged channels
   int* flag_counts = nullptr;    // [slot]
-  double* norm_moments = nullptr;  // [slot][2 * kVarChunks + 2]
+  double* norm_moments = nullptr;  // [slot][kNormMomentsDoubles]
   unsigned* norm_tickets = nullptr;  // [slot]
   int* host_flag_counts = nullptr;   // pinned [slot]
   double* host_norm = nullptr;       // pinned [2]: mean, std of search 0
@@ -173,7 +173,7 @@ void free_prec(sc_dd* d) {
   dfree(d, &d->top16, sizeof(float) * N * S);
   dfree(d, &d->flags, sizeof(int) * N * S);
   dfree(d, &d->flag_counts, sizeof(int) * S);
-  dfree(d, &d->norm_moments, sizeof(double) * (2 * scb::kVarChunks + 2) * S);
+  dfree(d, &d->norm_moments, sizeof(double) * scb::kNormMomentsDoubles * S);
   dfree(d, &d->norm_tickets, sizeof(unsigned) * S);
   if (d->host_flag_counts) cudaFreeHost(d->host_flag_counts);
   if (d->host_norm) cudaFreeHost(d->host_norm);
@@ -192,7 +192,7 @@ int ensure_prec(sc_dd* d, int slots) {
       (e = dalloc(d, &d->top16, sizeof(float) * N * S)) != cudaSuccess ||
       (e = dalloc(d, &d->flags, sizeof(int) * N * S)) != cudaSuccess ||
       (e = dalloc(d, &d->flag_counts, sizeof(int) * S)) != cudaSuccess ||
-      (e = dalloc(d, &d->norm_moments, sizeof(double) * (2 * scb::kVarChunks + 2) * S)) != cudaSuccess ||
+      (e = dalloc(d, &d->norm_moments, sizeof(double) * scb::kNormMomentsDoubles * S)) != cudaSuccess ||
       (e = dalloc(d, &d->norm_tickets, sizeof(unsigned) * S)) != cudaSuccess ||
       (e = cudaMallocHost(&d->host_flag_counts, sizeof(int) * S)) != cudaSuccess ||
       (e = cudaMallocHost(&d->host_norm, sizeof(double) * 2)) != cudaSuccess) {
@@ -306,7 +306,7 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
       q.top16 = dd->top16 + N * k;
       q.flags = dd->flags + N * k;
       q.flag_count = dd->flag_counts + k;
-      q.norm_moments = dd->norm_moments + (size_t)(2 * scb::kVarChunks + 2) * k;
+      q.norm_moments = dd->norm_moments + (size_t)scb::kNormMomentsDoubles * k;
       q.norm_ticket = dd->norm_tickets + k;
     }
   }

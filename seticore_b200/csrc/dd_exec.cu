@@ -243,7 +243,7 @@ size_t ExecSearch::scratch_bytes(int Tr, int N, int cand_cap, int n_partials, in
              a(sizeof(int) * order_list_entries(N)) + a(sizeof(SearchHeader)) + a(sizeof(Candidate) * cand_cap);
   if (elem != kElemF32) {
     b += a((size_t)2 * Tr * N) + a(sizeof(float) * N) + a(sizeof(int) * N) + a(sizeof(int)) +
-         a(sizeof(double) * (2 * kVarChunks + 2)) + a(sizeof(unsigned));
+         a(sizeof(double) * kNormMomentsDoubles) + a(sizeof(unsigned));
   }
   return b;
 }
@@ -279,7 +279,7 @@ void ExecSearch::carve(char* base, int n_partials) {
     flag_count = reinterpret_cast<int*>(p);
     p += a(sizeof(int));
     norm_moments = reinterpret_cast<double*>(p);
-    p += a(sizeof(double) * (2 * kVarChunks + 2));
+    p += a(sizeof(double) * kNormMomentsDoubles);
     norm_ticket = reinterpret_cast<unsigned*>(p);
   }
 }

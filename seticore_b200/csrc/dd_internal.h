@@ -9,6 +9,10 @@ namespace scb {
 constexpr int kMaxSeg = 4;       // staged windows per tree work item when jobs have their own rows
 constexpr int kMaxBatch = 64;    // searches per batched launch (descriptors travel as kernel parameters)
 constexpr int kVarChunks = 1024; // variance-emulation chunks per search, at most
+// The 16-bit forms' moments buffer per search (doubles): per-block sums [0, K), sums of
+// squares [K, 2K), then mean, standard deviation and the minimum of the unrounded rows at
+// 2K, 2K + 1, 2K + 2, then per-block minima [2K + 4, 3K + 4).
+constexpr int kNormMomentsDoubles = 3 * kVarChunks + 4;
 
 // Element types of a tree launch's input.
 constexpr int kElemF32 = 0;
@@ -222,7 +226,7 @@ struct PrecisionDesc {
   int T, Tr, N;         // unrounded and rounded timesteps, channels
   void* norm;           // normalised 16-bit copy [Tr][N] (dense)
   float* colsum;        // column sums of the float32 power, formed by the moments pass
-  double* moments;      // 2 * kVarChunks partial sums + [mean, std] at 2 * kVarChunks
+  double* moments;      // kNormMomentsDoubles: partial sums, [mean, std, min], partial minima
   unsigned* ticket;
   const float* top16;   // tops of the 16-bit tree (normalised units)
   const SearchHeader* hdr;
@@ -240,7 +244,8 @@ struct PrecisionBatch {
 };
 // FP64 mean and standard deviation of the unrounded rows, then the normalised copy.
 cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
-// Lists every channel whose 16-bit top reaches 0.9 x the threshold.
+// Lists every channel whose 16-bit top reaches the threshold less the rounding bound
+// (dd_precision.cu, flag_threshold): every channel whose exact top can reach it.
 cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream);
 // The exact float32 top of every listed channel: each eligible path summed from the
 // original power in the tree's pairing, the maximum floored at 0.

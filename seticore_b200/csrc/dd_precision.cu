@@ -1,24 +1,25 @@
 // The precision form: searches over normalised 16-bit spectra with exact hits.
 //
-//   1. norm_moments_kernel: per search, the FP64 mean and standard deviation of the
-//      unrounded rows of the original float32 power (zero-padded rows excluded), and in
-//      the same read the float32 column sums the statistics need.
+//   1. norm_moments_kernel: per search, the FP64 mean and standard deviation and the
+//      minimum of the unrounded rows of the original float32 power (zero-padded rows
+//      excluded), and in the same read the float32 column sums the statistics need.
 //   2. normalize_kernel: y = (x - mean) / std in FP64, rounded to BF16 or FP16 (padded
 //      rows stay 0), into a dense [Tr][N] 16-bit copy -- half the bytes of the input.
 //   3. (dd_tree.cu, dd_levels.cu) the tree over y, accumulating in FP32, gives approximate
 //      tops.  A path sum of y equals (P - T*mean) / std for the path sum P of x, so the
 //      order of path sums is kept up to the 16-bit rounding.
-//   4. flag_channels_kernel: lists every channel whose approximate top reaches 0.9 x the
-//      threshold in SNR units, P >= median + 0.9 * snr * std, mapped to y units.
+//   4. flag_channels_kernel: lists every channel whose approximate top reaches the flag
+//      threshold, the threshold mapped to y units less a bound on the rounding of the
+//      16-bit values and of both float trees (flag_threshold).
 //   5. recompute_direct_kernel (up to 16 rows: one thread per channel and drift block,
 //      all offsets from the subtree's leaves) or recompute_kernel (one path per thread):
 //      for each listed channel, every eligible path is summed from the original power in
 //      the tree's own pairing (bit-identical to the plain form's tree) and the maximum,
 //      floored at 0, becomes its top.  Every other channel keeps top 0:
-//      its approximate top is below 0.9 x threshold, so its exact top is below the
+//      its approximate top is below the flag threshold, so its exact top is below the
 //      threshold and it can neither become a window candidate nor beat one
 //      (dedoppler.cu:275-302 compares only with values above the threshold).  The hit list
-//      is therefore the plain form's.
+//      is therefore the plain form's, whatever the threshold or the data.
 // The statistics (median, standard deviation, threshold) always come from the float32
 // column sums, exactly as in the plain form.
 #include <cuda_bf16.h>
@@ -36,10 +37,11 @@ namespace {
 
 __global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
-  __shared__ double r1[32], r2[32];
+  __shared__ double r1[32], r2[32], r3[32];
   __shared__ bool last_block;
   const long long total = (long long)d.T * d.N;
   double s1 = 0.0, s2 = 0.0;
+  float mn = __int_as_float(0x7f800000);  // +inf; NaNs are skipped (and flag their channels)
   // Each thread takes columns (four at a time with 128-bit loads when the rows allow them)
   // down all Tr rows: the moments over the T loaded rows, and the column sums in row order
   // as a float sum (sumColumns, dedoppler.cu:63-72, bit-identical to colsum_kernel).
@@ -59,6 +61,7 @@ __global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
           const double a = v.x, b2 = v.y, c2 = v.z, e = v.w;
           s1 += (a + b2) + (c2 + e);
           s2 += (a * a + b2 * b2) + (c2 * c2 + e * e);
+          mn = fminf(mn, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
         }
       }
       if (d.colsum) reinterpret_cast<float4*>(d.colsum)[c] = cs;
@@ -72,6 +75,7 @@ __global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
         if (t < d.T) {
           s1 += (double)x;
           s2 += (double)x * (double)x;
+          mn = fminf(mn, x);
         }
       }
       if (d.colsum) d.colsum[c] = cs;
@@ -80,48 +84,58 @@ __global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
   for (int o = 16; o > 0; o >>= 1) {
     s1 += __shfl_down_sync(0xffffffffu, s1, o);
     s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    mn = fminf(mn, __shfl_down_sync(0xffffffffu, mn, o));
   }
   if ((threadIdx.x & 31) == 0) {
     r1[threadIdx.x >> 5] = s1;
     r2[threadIdx.x >> 5] = s2;
+    r3[threadIdx.x >> 5] = mn;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0.0, q = 0.0;
+    double a = 0.0, q = 0.0, m = r3[0];
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       a += r1[w];
       q += r2[w];
+      m = fmin(m, r3[w]);
     }
     d.moments[blockIdx.x] = a;
     d.moments[kVarChunks + blockIdx.x] = q;
+    d.moments[2 * kVarChunks + 4 + blockIdx.x] = m;
     __threadfence();
     last_block = (atomicAdd(d.ticket, 1u) == gridDim.x - 1);
   }
   __syncthreads();
   if (!last_block) return;
   __threadfence();
-  double a = 0.0, q = 0.0;
+  double a = 0.0, q = 0.0, m = __longlong_as_double(0x7ff0000000000000ll);
   for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
     a += __ldcg(d.moments + k);
     q += __ldcg(d.moments + kVarChunks + k);
+    m = fmin(m, __ldcg(d.moments + 2 * kVarChunks + 4 + k));
   }
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, o);
     q += __shfl_down_sync(0xffffffffu, q, o);
+    m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
   }
   __syncthreads();
   if ((threadIdx.x & 31) == 0) {
     r1[threadIdx.x >> 5] = a;
     r2[threadIdx.x >> 5] = q;
+    r3[threadIdx.x >> 5] = m;
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
   a = 0.0;
   q = 0.0;
+  m = r3[0];
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
     a += r1[w];
     q += r2[w];
+    m = fmin(m, r3[w]);
   }
+  d.moments[2 * kVarChunks + 2] = m;
   const double n = (double)total;
   const double mean = a / n;
   double var = q / n - mean * mean;
@@ -179,13 +193,46 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
   }
 }
 
+// The flag threshold in normalised path-sum units: every channel whose float32 top P_f
+// (the plain form's, tree order) reaches the search's threshold `thr` has an approximate
+// top S~ (the 16-bit tree's) of at least this value, so it is listed and recomputed.
+//
+// Rounding bounds, per path of the T unrounded rows (padded rows are 0 on both sides):
+//  * y_i = (x_i - mean) / std in FP64, then to float and to 16 bits: |y~_i - y_i| <= u |y_i|
+//    with u = 2^-8 + 2^-24 (BF16; 2^-11 + 2^-24 for FP16, plus an absolute 2^-25 below
+//    FP16's normal range, which covers its subnormals and its flush to zero).
+//  * float sums of n terms in the tree's pairwise order (depth L = log2 Tr): the error is
+//    at most g * sum|terms| with g = 1.01 L 2^-24, for both P_f and S~.
+//  * y_i >= -Ym with Ym = max(0, (mean - min x) / std), so sum|y_i| <= S_y + 2 T Ym along a
+//    path whose exact normalised sum is S_y = (P - T mean) / std; likewise
+//    sum|x_i| <= P + 2 T Xn with Xn = max(0, -min x).
+// If P_f >= thr then P >= a_x := thr - g (|thr| + 2 T Xn) (1 + 2g), i.e. S_y >= a =
+// (a_x - T mean) / std, and S~ >= S_y - c (|S_y| + 2 T Ym) - T e_abs with c = u + g (1 + u).
+// The right side grows with S_y (c < 1), so its value at S_y = a bounds S~ from below.
+// A margin of 2^-20 relative guards the double arithmetic here; NaN inputs and NaN tops are
+// always listed.
+__device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem) {
+  const double mean = d.moments[2 * kVarChunks], sd = d.moments[2 * kVarChunks + 1];
+  const double xmin = d.moments[2 * kVarChunks + 2];
+  const double thr = (double)d.hdr->threshold;
+  const int L = 31 - __clz(d.Tr);
+  const double g = 1.01 * L * 0x1p-24;
+  const bool fp16 = (elem == kElemF16);
+  const double u = (fp16 ? 0x1p-11 : 0x1p-8) + 0x1p-24;
+  const double e_abs = fp16 ? 0x1p-25 : 0.0;
+  const double T = (double)d.T;
+  const double xn = xmin < 0.0 ? -xmin : 0.0;
+  const double ym = fmax(0.0, (mean - xmin) / sd);
+  const double a_x = thr - g * (fabs(thr) + 2.0 * T * xn) * (1.0 + 2.0 * g);
+  const double a = (a_x - T * mean) / sd;
+  const double c = u + g * (1.0 + u);
+  const double lo = a - c * (fabs(a) + 2.0 * T * ym) - T * e_abs;
+  return (float)(lo - 0x1p-20 * (fabs(lo) + 1.0));
+}
+
 __global__ void flag_channels_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
-  // Loose threshold in SNR units (0.9 x), mapped to normalised path-sum units.
-  const double median = (double)d.hdr->median, sd = (double)d.hdr->std_dev;
-  const double mean = d.moments[2 * kVarChunks], scale = d.moments[2 * kVarChunks + 1];
-  const double thr_x = median + 0.9 * d.snr_threshold * sd;
-  const float thr_y = (float)((thr_x - (double)d.T * mean) / scale);
+  const float thr_y = flag_threshold(d, b.elem);
   const int lane = threadIdx.x & 31;
   for (int c0 = blockIdx.x * blockDim.x; c0 < d.N; c0 += gridDim.x * blockDim.x) {
     const int c = c0 + threadIdx.x;

@@ -110,3 +110,45 @@ def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle, name):
     print(json.dumps({"fp64_error_case": name, "shape": [spec.rounded_timesteps, spec.num_channels],
                       "drift_blocks": spec.num_drift_blocks(), "max_relative_top_error": err}))
     assert err["fp32"] < 1e-6
+
+
+def _bound_patterns():
+    rng = np.random.default_rng(77)
+    out = []
+    for T, N in ((16, 65536), (64, 20000)):
+        out.append((f"exponential_T{T}", rng.exponential(1.0, (T, N)).astype(np.float32)))
+        out.append((f"heavy_tail_T{T}", (rng.exponential(1.0, (T, N)) ** 4).astype(np.float32)))
+        x = rng.exponential(1.0, (T, N)).astype(np.float32)
+        x[:, rng.integers(0, N, 40)] += 200.0  # bright columns and lines
+        x[rng.integers(0, T, 30), rng.integers(0, N, 30)] += 1000.0
+        out.append((f"spiky_T{T}", x))
+        out.append((f"signed_T{T}", (rng.standard_normal((T, N)) * 5.0 - 1.0).astype(np.float32)))
+        out.append((f"offset_T{T}", (1e4 + rng.exponential(1.0, (T, N))).astype(np.float32)))
+    return out
+
+
+@pytest.mark.parametrize("name,x", _bound_patterns(), ids=[p[0] for p in _bound_patterns()])
+@pytest.mark.parametrize("precision", ["bf16", "fp16"])
+@pytest.mark.parametrize("snr", [3.0, 10.0])
+def test_flag_bound_covers_every_channel_at_the_threshold(torch_cuda, name, x, precision, snr):
+    """The flag threshold is a rounding bound, not a fixed margin: at any SNR threshold, on
+    noise, heavy tails, spikes, signed values and a large offset, every channel whose FP32
+    top reaches the threshold is listed and recomputed (its top in the 16-bit form equals the
+    FP32 top bit for bit), and the hit lists are identical."""
+    from seticore_b200 import Dedopplerer
+    T, N = x.shape
+    xt = torch_cuda.from_numpy(x).cuda()
+    dd = Dedopplerer(T, N, 2.7939677e-6, 18.253611 * 16 / T)
+    h32 = [(h.index, h.drift_steps, np.float32(h.power)) for h in dd.search_raw(xt, -1, 0, 4.0, 0.0, snr)]
+    top32 = dd.channel_array("top").cpu().numpy().copy()
+    thr = np.float32(dd.last_stats().threshold)
+    dd.set_precision(precision)
+    h16 = [(h.index, h.drift_steps, np.float32(h.power)) for h in dd.search_raw(xt, -1, 0, 4.0, 0.0, snr)]
+    top16 = dd.channel_array("top").cpu().numpy()
+    st = dd.last_stats()
+    dd.close()
+    assert np.float32(st.threshold) == thr
+    need = np.nonzero(top32 >= thr)[0]
+    np.testing.assert_array_equal(top16[need].view(np.uint32), top32[need].view(np.uint32))
+    assert h16 == h32
+    assert st.recomputed_channels >= len(need)
