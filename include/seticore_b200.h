@@ -65,8 +65,9 @@ typedef struct sc_dd_stats {
   int recomputed_channels; /* precision form: channels whose top was recomputed in FP32 */
   int total_channels;      /* channels of the search */
   int d2h_bytes;           /* bytes the whole call copied device -> host (headers, candidates) */
-  double norm_mean;       /* precision form: FP64 mean of the power, used to normalise */
-  double norm_std;        /* precision form: FP64 standard deviation, used to normalise */
+  double norm_mean;       /* precision form: the FP64 mean that normalised the power (of the
+                             first, middle and last unrounded rows) */
+  double norm_std;        /* precision form: the FP64 standard deviation used with it */
   int order_exact;        /* 1: median, mean and std_dev were formed in the order the
                              reference's std::nth_element calls leave the column sums, so they
                              are bit-identical to the reference's (searches whose 5 %, 50 % or

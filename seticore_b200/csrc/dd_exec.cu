@@ -86,7 +86,7 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
 
 // Searches whose column sums come with another pass over the input: the float32 tree of up
 // to 32 rows (its drift range always holds drift block 0: dmin <= 0 <= dmax), and the
-// 16-bit forms' moments pass.
+// 16-bit forms' normalising pass.
 bool tree_colsum(const ExecSearch& e) { return e.elem == kElemF32 && e.Tr <= 32 && e.dmin <= 0 && e.dmax >= 0; }
 bool fused_colsum(const ExecSearch& e) { return tree_colsum(e) || e.elem != kElemF32; }
 
@@ -158,8 +158,8 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       if (q.count && (e = normalize_batch(q, num_sms, stream)) != cudaSuccess) return e;
     }
     // Column sums: the float32 trees over up to 32 rows compute their own from the staged
-    // rows and the 16-bit forms in their moments pass; the level path reads the input once
-    // here.
+    // rows and the 16-bit forms in their normalising pass; the level path reads the input
+    // once here.
     {
       SearchBatch cb;
       cb.count = 0;

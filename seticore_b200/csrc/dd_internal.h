@@ -10,9 +10,10 @@ constexpr int kMaxSeg = 4;       // staged windows per tree work item when jobs 
 constexpr int kMaxBatch = 64;    // searches per batched launch (descriptors travel as kernel parameters)
 constexpr int kVarChunks = 1024; // variance-emulation chunks per search, at most
 // The 16-bit forms' moments buffer per search (doubles): per-block sums [0, K), sums of
-// squares [K, 2K), then mean, standard deviation and the minimum of the unrounded rows at
-// 2K, 2K + 1, 2K + 2, then per-block minima [2K + 4, 3K + 4).
-constexpr int kNormMomentsDoubles = 3 * kVarChunks + 4;
+// squares [K, 2K), then the normalisation's mean and standard deviation and the minimum and
+// maximum of the unrounded rows at 2K .. 2K + 3, then per-block (minimum, maximum) pairs
+// from 2K + 4.
+constexpr int kNormMomentsDoubles = 4 * kVarChunks + 4;
 
 // Element types of a tree launch's input.
 constexpr int kElemF32 = 0;
@@ -225,8 +226,8 @@ struct PrecisionDesc {
   long long row_stride;
   int T, Tr, N;         // unrounded and rounded timesteps, channels
   void* norm;           // normalised 16-bit copy [Tr][N] (dense)
-  float* colsum;        // column sums of the float32 power, formed by the moments pass
-  double* moments;      // kNormMomentsDoubles: partial sums, [mean, std, min], partial minima
+  float* colsum;        // column sums of the float32 power, formed by the normalising pass
+  double* moments;      // kNormMomentsDoubles: partials, [mean, std, min, max], partial extremes
   unsigned* ticket;
   const float* top16;   // tops of the 16-bit tree (normalised units)
   const SearchHeader* hdr;

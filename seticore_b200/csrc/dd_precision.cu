@@ -1,10 +1,11 @@
 // The precision form: searches over normalised 16-bit spectra with exact hits.
 //
-//   1. norm_moments_kernel: per search, the FP64 mean and standard deviation and the
-//      minimum of the unrounded rows of the original float32 power (zero-padded rows
-//      excluded), and in the same read the float32 column sums the statistics need.
-//   2. normalize_kernel: y = (x - mean) / std in FP64, rounded to BF16 or FP16 (padded
-//      rows stay 0), into a dense [Tr][N] 16-bit copy -- half the bytes of the input.
+//   1. norm_sample_kernel: per search, the FP64 mean and standard deviation of three of
+//      the unrounded rows (first, middle, last): the scale of the 16-bit values.
+//   2. normalize_kernel, one read of the original float32 power: y = (x - mean) / std in
+//      FP64, rounded to BF16 or FP16 (padded rows stay 0), into a dense [Tr][N] 16-bit copy
+//      -- half the bytes of the input -- and, in the same read, the float32 column sums the
+//      statistics need and the minimum and maximum of the unrounded rows.
 //   3. (dd_tree.cu, dd_levels.cu) the tree over y, accumulating in FP32, gives approximate
 //      tops.  A path sum of y equals (P - T*mean) / std for the path sum P of x, so the
 //      order of path sums is kept up to the 16-bit rounding.
@@ -35,114 +36,113 @@ namespace scb {
 
 namespace {
 
-__global__ void norm_moments_kernel(const __grid_constant__ PrecisionBatch b) {
-  const PrecisionDesc& d = b.s[blockIdx.y];
-  __shared__ double r1[32], r2[32], r3[32];
+// Block-wide reduction of (sum, sum of squares, min, max) into the search's moments
+// buffer: per-block partials, then the last block to arrive (a ticket) folds them.  Returns
+// true in thread 0 of that last block, with the totals in *a, *q, *mn, *mx.
+__device__ bool fold_moments(const PrecisionDesc& d, double s1, double s2, float mn, float mx, double* a, double* q,
+                             double* omn, double* omx) {
+  __shared__ double r1[32], r2[32], r3[32], r4[32];
   __shared__ bool last_block;
-  const long long total = (long long)d.T * d.N;
-  double s1 = 0.0, s2 = 0.0;
-  float mn = __int_as_float(0x7f800000);  // +inf; NaNs are skipped (and flag their channels)
-  // Each thread takes columns (four at a time with 128-bit loads when the rows allow them)
-  // down all Tr rows: the moments over the T loaded rows, and the column sums in row order
-  // as a float sum (sumColumns, dedoppler.cu:63-72, bit-identical to colsum_kernel).
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nth = (long long)gridDim.x * blockDim.x;
-  const bool vec = (d.N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
-  if (vec) {
-    for (long long c = tid; c < d.N / 4; c += nth) {
-      float4 cs = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (int t = 0; t < d.Tr; ++t) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(d.input + (long long)t * d.row_stride) + c);
-        cs.x += v.x;
-        cs.y += v.y;
-        cs.z += v.z;
-        cs.w += v.w;
-        if (t < d.T) {
-          const double a = v.x, b2 = v.y, c2 = v.z, e = v.w;
-          s1 += (a + b2) + (c2 + e);
-          s2 += (a * a + b2 * b2) + (c2 * c2 + e * e);
-          mn = fminf(mn, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
-        }
-      }
-      if (d.colsum) reinterpret_cast<float4*>(d.colsum)[c] = cs;
-    }
-  } else {
-    for (long long c = tid; c < d.N; c += nth) {
-      float cs = 0.0f;
-      for (int t = 0; t < d.Tr; ++t) {
-        const float x = __ldg(d.input + (long long)t * d.row_stride + c);
-        cs += x;
-        if (t < d.T) {
-          s1 += (double)x;
-          s2 += (double)x * (double)x;
-          mn = fminf(mn, x);
-        }
-      }
-      if (d.colsum) d.colsum[c] = cs;
-    }
-  }
   for (int o = 16; o > 0; o >>= 1) {
     s1 += __shfl_down_sync(0xffffffffu, s1, o);
     s2 += __shfl_down_sync(0xffffffffu, s2, o);
     mn = fminf(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, o));
   }
   if ((threadIdx.x & 31) == 0) {
     r1[threadIdx.x >> 5] = s1;
     r2[threadIdx.x >> 5] = s2;
     r3[threadIdx.x >> 5] = mn;
+    r4[threadIdx.x >> 5] = mx;
   }
   __syncthreads();
+  double* part = d.moments;  // sums [0, K), squares [K, 2K), minima and maxima from 2K + 4
   if (threadIdx.x == 0) {
-    double a = 0.0, q = 0.0, m = r3[0];
+    double x1 = 0.0, x2 = 0.0, m = r3[0], M = r4[0];
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      a += r1[w];
-      q += r2[w];
+      x1 += r1[w];
+      x2 += r2[w];
       m = fmin(m, r3[w]);
+      M = fmax(M, r4[w]);
     }
-    d.moments[blockIdx.x] = a;
-    d.moments[kVarChunks + blockIdx.x] = q;
-    d.moments[2 * kVarChunks + 4 + blockIdx.x] = m;
+    part[blockIdx.x] = x1;
+    part[kVarChunks + blockIdx.x] = x2;
+    part[2 * kVarChunks + 4 + 2 * blockIdx.x] = m;
+    part[2 * kVarChunks + 5 + 2 * blockIdx.x] = M;
     __threadfence();
     last_block = (atomicAdd(d.ticket, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (!last_block) return;
+  if (!last_block) return false;
   __threadfence();
-  double a = 0.0, q = 0.0, m = __longlong_as_double(0x7ff0000000000000ll);
+  double x1 = 0.0, x2 = 0.0, m = __longlong_as_double(0x7ff0000000000000ll), M = -m;
   for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
-    a += __ldcg(d.moments + k);
-    q += __ldcg(d.moments + kVarChunks + k);
-    m = fmin(m, __ldcg(d.moments + 2 * kVarChunks + 4 + k));
+    x1 += __ldcg(part + k);
+    x2 += __ldcg(part + kVarChunks + k);
+    m = fmin(m, __ldcg(part + 2 * kVarChunks + 4 + 2 * k));
+    M = fmax(M, __ldcg(part + 2 * kVarChunks + 5 + 2 * k));
   }
   for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    q += __shfl_down_sync(0xffffffffu, q, o);
+    x1 += __shfl_down_sync(0xffffffffu, x1, o);
+    x2 += __shfl_down_sync(0xffffffffu, x2, o);
     m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    M = fmax(M, __shfl_down_sync(0xffffffffu, M, o));
   }
   __syncthreads();
   if ((threadIdx.x & 31) == 0) {
-    r1[threadIdx.x >> 5] = a;
-    r2[threadIdx.x >> 5] = q;
+    r1[threadIdx.x >> 5] = x1;
+    r2[threadIdx.x >> 5] = x2;
     r3[threadIdx.x >> 5] = m;
+    r4[threadIdx.x >> 5] = M;
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
-  a = 0.0;
-  q = 0.0;
+  if (threadIdx.x != 0) return false;
+  x1 = 0.0;
+  x2 = 0.0;
   m = r3[0];
+  M = r4[0];
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-    a += r1[w];
-    q += r2[w];
+    x1 += r1[w];
+    x2 += r2[w];
     m = fmin(m, r3[w]);
+    M = fmax(M, r4[w]);
   }
-  d.moments[2 * kVarChunks + 2] = m;
-  const double n = (double)total;
+  *d.ticket = 0;
+  *a = x1;
+  *q = x2;
+  *omn = m;
+  *omx = M;
+  return true;
+}
+
+// The normalisation's mean and standard deviation, in FP64, from a sample of the unrounded
+// rows: the first, middle and last.  Exactness does not depend on them (the flag bound uses
+// whatever they are); they only set the 16-bit values' scale.
+__global__ void norm_sample_kernel(const __grid_constant__ PrecisionBatch b) {
+  const PrecisionDesc& d = b.s[blockIdx.y];
+  const int rows[3] = {0, d.T / 2, d.T - 1};
+  const int nrows = d.T >= 3 ? 3 : d.T;
+  double s1 = 0.0, s2 = 0.0;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  for (int r = 0; r < nrows; ++r) {
+    const float* row = d.input + (long long)rows[r] * d.row_stride;
+    for (long long c = tid; c < d.N; c += nth) {
+      const double x = __ldg(row + c);
+      if (x == x) {  // NaNs do not enter the scale
+        s1 += x;
+        s2 += x * x;
+      }
+    }
+  }
+  double a, q, mn, mx;
+  if (!fold_moments(d, s1, s2, 0.0f, 0.0f, &a, &q, &mn, &mx)) return;
+  const double n = (double)nrows * d.N;
   const double mean = a / n;
   double var = q / n - mean * mean;
-  if (!(var > 0.0)) var = 1.0;  // constant input: any positive scale keeps the order
-  d.moments[2 * kVarChunks] = mean;
+  if (!(var > 0.0) || !(mean == mean)) var = 1.0;  // constant sample: any positive scale keeps the order
+  d.moments[2 * kVarChunks] = (mean == mean) ? mean : 0.0;
   d.moments[2 * kVarChunks + 1] = sqrt(var);
-  *d.ticket = 0;
 }
 
 template <typename E>
@@ -156,6 +156,11 @@ __device__ __forceinline__ __half from_float<__half>(float v) {
   return __float2half_rn(v);
 }
 
+// One read of the original power: y = (x - mean) / std in FP64, rounded to BF16 or FP16, into
+// the dense [Tr][N] 16-bit copy (padded rows 0); in the same read the float32 column sums in
+// row order (sumColumns, dedoppler.cu:63-72, bit-identical to colsum_kernel) and the minimum
+// and maximum of the unrounded rows, which the flag bound needs.  A thread takes four
+// columns (one with unaligned rows) down all Tr rows.
 template <typename E>
 __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
@@ -164,33 +169,53 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
   E* out = static_cast<E*>(d.norm);
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
+  float mn = __int_as_float(0x7f800000), mx = -mn;  // NaNs are skipped (they flag themselves)
   const bool vec = (d.N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
-  for (int t = 0; t < d.Tr; ++t) {
-    const float* row = d.input + (long long)t * d.row_stride;
-    E* orow = out + (long long)t * d.N;
-    if (vec) {
-      const float4* r4 = reinterpret_cast<const float4*>(row);
-      for (long long c = tid; c < d.N / 4; c += nth) {
+  if (vec) {
+    for (long long c = tid; c < d.N / 4; c += nth) {
+      float4 cs = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int t = 0; t < d.Tr; ++t) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(d.input + (long long)t * d.row_stride) + c);
+        cs.x += v.x;
+        cs.y += v.y;
+        cs.z += v.z;
+        cs.w += v.w;
         E y[4] = {from_float<E>(0.0f), from_float<E>(0.0f), from_float<E>(0.0f), from_float<E>(0.0f)};
         if (t < d.T) {
-          const float4 v = __ldg(r4 + c);
           y[0] = from_float<E>((float)(((double)v.x - mean) * inv));
           y[1] = from_float<E>((float)(((double)v.y - mean) * inv));
           y[2] = from_float<E>((float)(((double)v.z - mean) * inv));
           y[3] = from_float<E>((float)(((double)v.w - mean) * inv));
+          mn = fminf(mn, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
+          mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
         }
         uint2 packed;
         memcpy(&packed, y, sizeof(packed));
-        reinterpret_cast<uint2*>(orow)[c] = packed;
+        reinterpret_cast<uint2*>(out + (long long)t * d.N)[c] = packed;
       }
-    } else {
-      for (long long c = tid; c < d.N; c += nth) {
+      if (d.colsum) reinterpret_cast<float4*>(d.colsum)[c] = cs;
+    }
+  } else {
+    for (long long c = tid; c < d.N; c += nth) {
+      float cs = 0.0f;
+      for (int t = 0; t < d.Tr; ++t) {
+        const float x = __ldg(d.input + (long long)t * d.row_stride + c);
+        cs += x;
         float y = 0.0f;
-        if (t < d.T) y = (float)(((double)__ldg(row + c) - mean) * inv);
-        orow[c] = from_float<E>(y);
+        if (t < d.T) {
+          y = (float)(((double)x - mean) * inv);
+          mn = fminf(mn, x);
+          mx = fmaxf(mx, x);
+        }
+        out[(long long)t * d.N + c] = from_float<E>(y);
       }
+      if (d.colsum) d.colsum[c] = cs;
     }
   }
+  double a, q, omn, omx;
+  if (!fold_moments(d, 0.0, 0.0, mn, mx, &a, &q, &omn, &omx)) return;
+  d.moments[2 * kVarChunks + 2] = omn;
+  d.moments[2 * kVarChunks + 3] = omx;
 }
 
 // The flag threshold in normalised path-sum units: every channel whose float32 top P_f
@@ -213,7 +238,7 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
 // always listed.
 __device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem) {
   const double mean = d.moments[2 * kVarChunks], sd = d.moments[2 * kVarChunks + 1];
-  const double xmin = d.moments[2 * kVarChunks + 2];
+  const double xmin = d.moments[2 * kVarChunks + 2], xmax = d.moments[2 * kVarChunks + 3];
   const double thr = (double)d.hdr->threshold;
   const int L = 31 - __clz(d.Tr);
   const double g = 1.01 * L * 0x1p-24;
@@ -227,6 +252,10 @@ __device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem
   const double a = (a_x - T * mean) / sd;
   const double c = u + g * (1.0 + u);
   const double lo = a - c * (fabs(a) + 2.0 * T * ym) - T * e_abs;
+  // Normalised values beyond the 16-bit range (a scale from an unrepresentative sample)
+  // void the relative bounds: then every channel is listed.
+  const double ymax = fmax(fabs(xmax - mean), fabs(xmin - mean)) / sd;
+  if (!(ymax < (fp16 ? 60000.0 : 1e38))) return __int_as_float(0xff800000);  // -inf
   return (float)(lo - 0x1p-20 * (fabs(lo) + 1.0));
 }
 
@@ -321,9 +350,11 @@ cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
   int blocks = (4 * num_sms + b.count - 1) / b.count;
   if (blocks < 8) blocks = 8;
   if (blocks > kVarChunks) blocks = kVarChunks;
-  norm_moments_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
+  norm_sample_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
+  // At most kVarChunks blocks per search (the partials of the minimum and maximum).
   int nb = (8 * num_sms + b.count - 1) / b.count;
   if (nb < 8) nb = 8;
+  if (nb > kVarChunks) nb = kVarChunks;
   if (b.elem == kElemBF16) normalize_kernel<__nv_bfloat16><<<dim3(nb, b.count), 256, 0, stream>>>(b);
   else normalize_kernel<__half><<<dim3(nb, b.count), 256, 0, stream>>>(b);
   return cudaGetLastError();
