@@ -52,10 +52,12 @@ TREE_WARP_INSTR = 744.2e6 / 4
 # Level path of the beams workload, DRAM bytes per beam of 256 x 131072 (2 drift blocks):
 # direct16x4_kernel 268.5 + 223.2 MB and the last level 269.5 + 3.8 MB (ncu, one launch each).
 BEAMS_DRAM_BYTES = 765.0e6
-# Kernels of one FP32 batch of up to 64 searches of at most 32 rows: clear, tree, range,
-# three histogram passes, compaction, order-statistic finish, two variance kernels, window,
-# drift recovery.
-LAUNCHES_PER_BATCH = 12
+# Kernels of one FP32 batch of up to 64 searches of 2^20 channels and at most 32 rows (the
+# launch list of one node step, profiles/launch_list_node.md): clear, tree, range, three
+# histogram passes, compaction, order-statistic finish, two variance kernels, window, drift
+# recovery, and the exact statistics' launches, which exit at once when no search needs them
+# (reset, init, 15 partition rounds of three launches, two finishers, moments).
+LAUNCHES_PER_BATCH = 62
 
 
 def dist_setup():
@@ -634,8 +636,7 @@ def main():
                        "l2": "inputs (4.3 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
             "clocks": clk, "roofline": roofline, "e2e": e2e,
             "precision_forms": precision,
-            # per batch of up to 64 coarse channels: clear, tree (with the column sums), four
-            # select passes, moments, two variance kernels, window and resolve
+            # per batch of up to 64 coarse channels (LAUNCHES_PER_BATCH)
             "gpu_launches": len(tree_ms) * LAUNCHES_PER_BATCH * ((n_coarse + 63) // 64),
             "hits_per_step": hits_per_step[-1]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

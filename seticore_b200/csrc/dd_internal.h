@@ -212,10 +212,10 @@ inline long long level_row_length(int N) {
   const long long w = tree_tile_width();
   return (N + w - 1) / w * w;
 }
-// The slack of each row covers the stripe passes' per-row channel origins and shears
-// (one drift block of a last level of up to 16 rows, dd_levels.cu), so a whole row always
-// fits one pass.
-constexpr long long kLevelRowSlack = 1408;
+// The slack of each row covers the stripe passes' per-row channel origins and shears (up to
+// four drift blocks of a last level of up to 16 rows, dd_levels.cu), so the two level
+// buffers hold a whole-row pass of two drift blocks.
+constexpr long long kLevelRowSlack = 2048;
 inline size_t level_buffer_floats(int Tr, int N) {
   return (size_t)Tr * (size_t)(level_row_length(N) + kLevelRowSlack);
 }

@@ -338,17 +338,46 @@ cudaError_t stripes_search(const float* input, long long row_stride, int Tr, int
   const long long Nt = ((long long)N + 1055) / 1056 * 1056;
   const long long l2 = (long long)(level_l2_bytes() / sizeof(float));
   const long long budget = l2 > 0 ? std::min(l2, cap) : cap;
-  int J = std::min(ndb, std::min(kMaxBatch, level_max_chunk()));
-  long long L = 0;
-  for (;; J = (J + 1) / 2) {
-    const long long avail = budget / ((long long)J * Tr) - stripe_row_length(0, J, fr);
+  // Drift blocks per pass (J) and stripe length (L).  Whole-row mode: the fewest passes,
+  // ceil(ndb / J) x stripes, counting a narrow remainder stripe as a full pass (each pass
+  // costs a launch's fill and drain), the larger J on a tie, and stripes of equal length.
+  // With an L2 budget: the largest J whose stripes span at least four stripe units.
+  int J = 0;
+  long long L = 0, best_passes = -1;
+  for (int j = std::min(ndb, std::min(kMaxBatch, level_max_chunk()));; j = (j + 1) / 2) {
+    const long long avail = budget / ((long long)j * Tr) - stripe_row_length(0, j, fr);
+    long long lj = 0, stripes = 0;
     if (avail >= Nt) {
-      L = Nt;
-      break;
+      lj = Nt;
+      stripes = 1;
+    } else {
+      const long long lmax = std::max<long long>(0, avail) / kStripeUnit * kStripeUnit;
+      if (lmax >= kStripeUnit) {
+        stripes = (N + lmax - 1) / lmax;
+        lj = ((N + stripes - 1) / stripes + kStripeUnit - 1) / kStripeUnit * kStripeUnit;
+      }
     }
-    // at least four stripe units per pass unless one drift block is left
-    L = std::max<long long>(0, avail) / kStripeUnit * kStripeUnit;
-    if (L >= 4 * kStripeUnit || J == 1) break;
+    if (stripes > 0) {
+      if (l2 > 0) {
+        if (lj >= std::min<long long>(Nt, 4 * kStripeUnit) || j == 1) {
+          J = j;
+          L = lj;
+          break;
+        }
+      } else {
+        const long long passes = (long long)((ndb + j - 1) / j) * stripes;
+        if (best_passes < 0 || passes < best_passes) {
+          best_passes = passes;
+          J = j;
+          L = lj;
+        }
+      }
+    }
+    if (j == 1) break;
+  }
+  if (J == 0) {  // no stripe fits the budget: the smallest one, one drift block per pass
+    J = 1;
+    L = std::min<long long>(kStripeUnit, Nt);
   }
   if (L < Nt) L = std::min<long long>(std::max<long long>(L, kStripeUnit), Nt);
   long long Lp = stripe_row_length(L, J, fr);
