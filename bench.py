@@ -49,9 +49,10 @@ TREE_DRAM_BYTES = 78829184
 # Warp instructions the tree kernel executes per coarse channel of the node (ncu
 # smsp__inst_executed.sum of the same capture: 744.2 M for 4 coarse channels).
 TREE_WARP_INSTR = 744.2e6 / 4
-# Level path of the beams workload, DRAM bytes per beam of 256 x 131072 (2 drift blocks):
-# direct16x4_kernel 268.5 + 223.2 MB and the last level 269.5 + 3.8 MB (ncu, one launch each).
-BEAMS_DRAM_BYTES = 765.0e6
+# Level path of the beams workload, DRAM bytes per beam of 256 x 131072 (2 drift blocks, one
+# whole-row pass): the emitting first level 134.3 + 213.1 MB and the last level 269.5 + 3.9 MB
+# (ncu, one launch each; profiles/level_kernels_beams.md).
+BEAMS_DRAM_BYTES = 620.7e6
 # Kernels of one FP32 batch of up to 64 searches of 2^20 channels and at most 32 rows (the
 # launch list of one node step, profiles/launch_list_node.md): clear, tree, range, three
 # histogram passes, compaction, order-statistic finish, two variance kernels, window, drift
@@ -140,10 +141,10 @@ def bytes_fused_fp32(Tr, n):
 
 
 def bytes_fused_16bit(Tr, n):
-    """What the 16-bit forms must move per search: the float32 input read by the moments pass
-    and again by normalisation, the 16-bit copy written and read once by the tree, and the
-    per-channel tops and column sums: 4*Tr*N*2 + 2*Tr*N*2 + 8*N."""
-    return 12 * Tr * n + 8 * n
+    """What the 16-bit forms must move per search: the float32 input read once by the
+    normalising pass (plus three sampled rows for its scale), the 16-bit copy written and read
+    once by the tree, and the per-channel tops and column sums: 4*Tr*N + 12*N + 2*Tr*N*2 + 8*N."""
+    return 8 * Tr * n + 20 * n
 
 
 def num_sms():
@@ -534,8 +535,8 @@ def main():
         precision[prec] = {"value": world * samples_per_step / (p_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": p_ms,
                            "hbm_frac_of_step": alg16 / (p_ms / 1e3) / 1e9 / peak16,
                            "bytes_per_step": alg16,
-                           "bytes_per_step_note": "moments read + normalise read/write + one 16-bit tree read "
-                                                  "+ tops and column sums (12*Tr*N + 8*N per search)",
+                           "bytes_per_step_note": "three sampled rows + one normalising read/write + one 16-bit "
+                                                  "tree read + tops and column sums (8*Tr*N + 20*N per search)",
                            "hits_identical_to_fp32": identical,
                            "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}",
                            "speedup_vs_fp32": ms / p_ms}

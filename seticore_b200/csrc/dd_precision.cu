@@ -125,13 +125,27 @@ __global__ void norm_sample_kernel(const __grid_constant__ PrecisionBatch b) {
   double s1 = 0.0, s2 = 0.0;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
+  const bool vec = (d.N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
   for (int r = 0; r < nrows; ++r) {
     const float* row = d.input + (long long)rows[r] * d.row_stride;
-    for (long long c = tid; c < d.N; c += nth) {
-      const double x = __ldg(row + c);
-      if (x == x) {  // NaNs do not enter the scale
-        s1 += x;
-        s2 += x * x;
+    if (vec) {
+      for (long long c = tid; c < d.N / 4; c += nth) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(row) + c);
+        const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (e[i] == e[i]) {  // NaNs do not enter the scale
+            s1 += (double)e[i];
+            s2 += (double)e[i] * (double)e[i];
+          }
+      }
+    } else {
+      for (long long c = tid; c < d.N; c += nth) {
+        const double x = __ldg(row + c);
+        if (x == x) {
+          s1 += x;
+          s2 += x * x;
+        }
       }
     }
   }
@@ -347,9 +361,8 @@ __global__ void recompute_kernel(const __grid_constant__ PrecisionBatch b) {
 
 cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream) {
   if (b.count <= 0) return cudaSuccess;
-  int blocks = (4 * num_sms + b.count - 1) / b.count;
-  if (blocks < 8) blocks = 8;
-  if (blocks > kVarChunks) blocks = kVarChunks;
+  // About 64 sampled values per thread (three rows), at most kVarChunks blocks per search.
+  int blocks = (int)std::min<long long>(kVarChunks, std::max<long long>(8, (3ll * b.maxN + 16383) / 16384));
   norm_sample_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
   // At most kVarChunks blocks per search (the partials of the minimum and maximum).
   int nb = (8 * num_sms + b.count - 1) / b.count;
