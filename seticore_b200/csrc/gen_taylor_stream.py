@@ -19,8 +19,9 @@ fills every node's window for the first channel, the loop body is straight-line 
 U channels, and the values a later iteration still needs are carried in registers across
 the back edge.  Looping (rather than unrolling the whole strip) keeps the code of one
 offset half small enough for the instruction cache.  Each channel's outputs are folded into
-a running maximum (starting at 0, so NaN and negative sums never count) that fold_max()
-merges into the CTA's per-channel maxima in shared memory.  The emitting form
+a running maximum (starting at 0, so NaN and negative sums never count) that the caller's
+fold merges into the CTA's per-channel maxima in shared memory: every channel, or only the
+channels whose paths are all eligible where the band's edges exclude some.  The emitting form
 (taylor_strip_emit) hands every root value to a sink instead: the first level of a tree of
 more than 32 rows, whose output planes the next level reads.
 """
@@ -163,7 +164,7 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
             else:
                 body.append((s, R + 1, f"    {acc} = fmaxf({acc}, o{s}_{i});"))
                 i += 1
-        body.append((s, R + 2, f"    fold_max(mrow + base + {s}, {acc});"))
+        body.append((s, R + 2, f"    fold(mrow, base + {s}, {acc});"))
     body.sort(key=lambda x: (x[0], x[1]))
     lines += [t for _, _, t in body]
     # carry: new state k holds position U + mn + k
@@ -181,8 +182,9 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
         return (f"template <typename Row, typename Sink>\n"
                 f"__device__ __forceinline__ void taylor_strip_emit_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
                 f"    const Row (&row)[{R}], Sink& sink) {{\n{body_text}\n}}\n")
-    return (f"template <typename Row>\n__device__ __forceinline__ void {loop_name(R, lo, hi, U, ITERS, reload)}(\n"
-            f"    const Row (&row)[{R}], float* __restrict__ mrow) {{\n{body_text}\n}}\n")
+    return (f"template <typename Row, typename Fold>\n__device__ __forceinline__ void "
+            f"{loop_name(R, lo, hi, U, ITERS, reload)}(\n"
+            f"    const Row (&row)[{R}], float* __restrict__ mrow, const Fold& fold) {{\n{body_text}\n}}\n")
 
 
 def loop_name(R, lo, hi, U, ITERS, reload=0):
@@ -267,16 +269,18 @@ def main(out_path):
         for k in range(nparts):
             parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, emit=True))
 
-    # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS, RELOAD>(row, mrow) for any element accessor.
-    parts.append("template <int R, int LO, int HI, int U, int ITERS, int RELOAD = 0, typename Row>\n"
-                 "__device__ __forceinline__ void taylor_strip_loop(const Row (&row)[R], float* __restrict__ mrow) {")
+    # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS, RELOAD>(row, mrow, fold) for any element
+    # accessor and fold (which merges a channel's maximum: all channels, or a range of them).
+    parts.append("template <int R, int LO, int HI, int U, int ITERS, int RELOAD = 0, typename Row, typename Fold>\n"
+                 "__device__ __forceinline__ void taylor_strip_loop(const Row (&row)[R], float* __restrict__ mrow, "
+                 "const Fold& fold) {")
     for R, nparts, U, IT, *rl in LOOP_CONFIGS:
         step = R // nparts
         rel = rl[0] if rl else 0
         for k in range(nparts):
             lo, hi = k * step, (k + 1) * step
             parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT} && "
-                         f"RELOAD == {rel}) {loop_name(R, lo, hi, U, IT, rel)}(row, mrow);")
+                         f"RELOAD == {rel}) {loop_name(R, lo, hi, U, IT, rel)}(row, mrow, fold);")
     parts.append("}")
     parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row, typename Sink>\n"
                  "__device__ __forceinline__ void taylor_strip_emit(const Row (&row)[R], Sink& sink) {")

@@ -46,7 +46,7 @@ def _translate(code):
         s = re.sub(r"^const (?:float|int) ", "", s)
         s = re.sub(r"^float ", "", s)
         s = s.replace("0.0f", "F0")
-        m = re.match(r"fold_max\(mrow \+ (.*), (\w+)\)$", s)
+        m = re.match(r"fold\(mrow, (.*), (\w+)\)$", s)
         if m:
             s = f"fold({m.group(1)}, {m.group(2)})"
         m = re.match(r"sink\.put\((\d+), (.*), (.*)\)$", s)
