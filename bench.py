@@ -43,12 +43,13 @@ MAX_DRIFT, MIN_DRIFT, SNR = 4.0, 0.0, 10.0
 METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 286.21 MB +
-# 29.11 MB); a launch covering k coarse channels moves k times this.
-TREE_DRAM_BYTES = 78829184
+# dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.93 MB +
+# 27.68 MB; profiles/tree_max_kernel_node.md); a launch covering k coarse channels moves k
+# times this.
+TREE_DRAM_BYTES = 78400384
 # Warp instructions the tree kernel executes per coarse channel of the node (ncu
-# smsp__inst_executed.sum of the same capture: 744.2 M for 4 coarse channels).
-TREE_WARP_INSTR = 744.2e6 / 4
+# smsp__inst_executed.sum of the same capture: 748.2 M for 4 coarse channels).
+TREE_WARP_INSTR = 748.2e6 / 4
 # Level path of the beams workload, DRAM bytes per beam of 256 x 131072 (2 drift blocks, one
 # whole-row pass): the emitting first level 134.3 + 213.1 MB and the last level 269.5 + 3.9 MB
 # (ncu, one launch each; profiles/level_kernels_beams.md).
