@@ -324,3 +324,29 @@ def test_staging_wait_give_up_is_reported(torch_cuda, port_oracle):
                                          arrays=True)
     np.testing.assert_array_equal(top, arrays["top"])
     assert [(h.index, h.drift_steps) for h in got] == [(h["index"], h["drift_steps"]) for h in want]
+
+
+EDGE_CASES = [
+    # T, N, max_drift (Hz/s at foff 2.79 Hz, tsamp 18.25 * 16 / T s): most strips sit near an
+    # edge of the band, where the drift blocks reach past it
+    (2, 1500, 40.0), (4, 2100, 30.0), (8, 2900, 25.0), (16, 3300, 20.0), (16, 1056, 12.0),
+    (32, 4000, 10.0), (32, 1200, 6.0), (13, 2500, 18.0), (64, 5000, 8.0),
+]
+
+
+@pytest.mark.parametrize("case", EDGE_CASES, ids=lambda c: f"T{c[0]}_N{c[1]}_md{c[2]}")
+def test_edge_strips_match_oracle(torch_cuda, port_oracle, case):
+    """Edge strips (channels near the band's ends whose drift blocks reach past it): the
+    generated tree with a range fold for the channels whose paths are all eligible, one path
+    at a time for the partially eligible ones.  Top sums bit-identical to the oracle."""
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    T, N, md = case
+    spec = SearchSpec(T, N, tsamp=18.253611 * 16 / max(T, 16), max_drift=md, seed=700 + T, n_tones=3,
+                      tone_drift=4.0, snr_threshold=8.0)
+    x = make_filterbank_numpy(spec)
+    want, wstats, arrays = port_oracle.search(x, spec.foff_mhz, spec.tsamp, md, 0.0, 8.0, arrays=True)
+    got, gstats, top, colsum = run_gpu(torch_cuda, x, spec.foff_mhz, spec.tsamp, md, 0.0, 8.0, T=T)
+    assert wstats["window_size"] > 0 and spec.num_drift_blocks() >= 3
+    np.testing.assert_array_equal(top, arrays["top"])
+    ties = compare_hits(got, want, gstats.threshold, wstats["threshold"], label=str(case))
+    assert len(ties) <= 1, ties
