@@ -9,16 +9,18 @@
 // k + (M1*...*Mk)*db and final offsets 16k + r, so the last level is one launch of the
 // fused max kernel over all problems (dd_tree.cu, one staged window per problem).
 //
-// The default levels are emit_kernel's 4- and 2-row sums (one thread per channel,
-// coalesced).  A plan may instead start with the emitting form of the fused tree
-// (M = 16): each CTA stages a tile of 16 rows once for two drift blocks and writes all 16
-// in-block offsets of every channel, which moves the least data (one staged read of the
-// input per pair of drift blocks, one write and one read of the planes per drift block)
-// but stores each lane's strip with a 33-float stride, so its writes reach L2 as partial
-// sectors.  Measured on 64 x 256 x 131072 it ran at 41 Gsamples/s against 72 for the
-// default, so only the pool's autotuner, which times both per shape, may pick it.  The
-// pairing of the adds is the tree's own at every level, so every path sum is
-// bit-identical to the reference's twoStageTaylorTree (taylor.cu:298-327).
+// Default splits:
+//  * Tr = 64, 128, 256, float rows: one 16-row level, the emitting form of the fused tree
+//    (dd_tree.cu; each CTA stages a 16-row group once for the pass's drift blocks and writes
+//    the 16 in-block offsets of a 352-channel strip through a shared buffer as whole bulk
+//    rows), then the last level over the 16 sub-problems.  Both run in passes of drift
+//    blocks and channels (stripes_search): the planes hold, per block row, only the channels
+//    the last level reads in that row (each block row has its own channel origin).
+//  * 16-bit rows and Tr > 256: direct16x4_kernel (four channels per thread from global
+//    memory), then emit_kernel's 4- and 2-row levels while more than 16 rows remain.
+// The pool's autotuner times these against the other splits per shape class.  The pairing
+// of the adds is the tree's own at every level, so every path sum is bit-identical to the
+// reference's twoStageTaylorTree (taylor.cu:298-327).
 #include <algorithm>
 #include <atomic>
 #include <cstdlib>
