@@ -27,7 +27,10 @@ def _hits(dd, xt, spec):
 
 CASES = [(16, 65536, 4.0, 1, 1), (16, 40000, 4.0, 2, 0), (8, 30000, 2.0, 3, 2), (13, 20000, 3.0, 4, 1),
          (4, 50000, 1.0, 5, 1), (2, 20000, 1.0, 6, 0), (16, 1 << 20, 4.0, 7, 2),
-         (32, 65536, 4.0, 8, 1), (100, 32768, 2.0, 9, 0), (256, 131072, 2.0, 10, 1)]
+         (32, 65536, 4.0, 8, 1), (100, 32768, 2.0, 9, 0), (256, 131072, 2.0, 10, 1),
+         # rows of a length that is not a whole number of 16-byte chunks: no bulk copy can take
+         # them, so they are staged by per-thread loads
+         (16, 30001, 4.0, 11, 1), (32, 12345, 3.0, 12, 0)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"T{c[0]}_N{c[1]}_s{c[3]}")
