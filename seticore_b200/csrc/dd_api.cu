@@ -19,6 +19,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "dd_common.cuh"
@@ -126,6 +127,20 @@ struct sc_dd {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, tree start/end, call end
   sc_dd_stats last{};
   bool have_last = false;
+  // CUDA graphs of repeated batches (same inputs, drift plan, threshold, form and settings):
+  // captured on the second sight, replayed afterwards.  Any reallocation of the scratch bumps
+  // `generation`, which is part of the key, and drops the graphs.
+  struct Graph {
+    uint64_t key;
+    cudaGraphExec_t exec;
+    unsigned long long last_use;
+  };
+  std::vector<Graph> graphs;
+  std::unordered_map<uint64_t, int> seen;  // sightings per key; -1: not capturable
+  unsigned long long clock = 0;
+  unsigned generation = 0;
+  cudaStream_t cap_stream = nullptr;
+  cudaEvent_t evj = nullptr;
 
   scb::SearchHeader* host_hdrs() { return static_cast<scb::SearchHeader*>(host); }
   scb::Candidate* host_cands() {
@@ -149,6 +164,13 @@ void dfree(sc_dd* d, T** p, size_t bytes) {
     d->device_bytes -= bytes;
     *p = nullptr;
   }
+}
+
+void drop_graphs(sc_dd* d) {
+  for (auto& g : d->graphs) cudaGraphExecDestroy(g.exec);
+  d->graphs.clear();
+  d->seen.clear();
+  ++d->generation;
 }
 
 void free_slots(sc_dd* d) {
@@ -185,6 +207,7 @@ void free_prec(sc_dd* d) {
 int ensure_prec(sc_dd* d, int slots) {
   if (slots <= d->prec_slots) return SC_DD_OK;
   cudaDeviceSynchronize();
+  drop_graphs(d);
   free_prec(d);
   const size_t S = slots, N = d->N;
   cudaError_t e;
@@ -207,6 +230,11 @@ int ensure_prec(sc_dd* d, int slots) {
 }
 
 void free_all(sc_dd* d) {
+  drop_graphs(d);
+  if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
+  if (d->evj) cudaEventDestroy(d->evj);
+  d->cap_stream = nullptr;
+  d->evj = nullptr;
   free_slots(d);
   free_prec(d);
   d->scratch_b = nullptr;  // inside scratch_a's allocation
@@ -224,6 +252,7 @@ int ensure_slots(sc_dd* d, int slots, int cand_cap) {
   const int ns = std::max(slots, d->slots);
   const int nc = std::max(cand_cap, d->cand_cap);
   cudaDeviceSynchronize();  // the old slots may still be in use by queued work
+  drop_graphs(d);
   free_slots(d);
   d->cand_cap = nc;
   const size_t N = d->N, S = ns;
@@ -313,16 +342,83 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
   EventHooks eh{dd, first_batch};
   scb::ExecHooks hooks;
   hooks.ctx = &eh;
+  // External event-record nodes when captured into a graph, so that the tree's time stays
+  // measurable from the host on every replay.
   hooks.before_tree = [](void* c, cudaStream_t st) {
     EventHooks* h = static_cast<EventHooks*>(c);
-    if (h->record) cudaEventRecord(h->dd->ev[1], st);
+    if (h->record && cudaEventRecordWithFlags(h->dd->ev[1], st, cudaEventRecordExternal) != cudaSuccess)
+      cudaGetLastError();
   };
   hooks.after_tree = [](void* c, cudaStream_t st) {
     EventHooks* h = static_cast<EventHooks*>(c);
-    if (h->record) cudaEventRecord(h->dd->ev[2], st);
+    if (h->record && cudaEventRecordWithFlags(h->dd->ev[2], st, cudaEventRecordExternal) != cudaSuccess)
+      cudaGetLastError();
   };
   cudaError_t e = scb::exec_queue(es, n, dd->scratch_a, dd->scratch_b, dd->num_sms, stream, hooks);
   if (e != cudaSuccess) return cuda_fail(e, "search kernels");
+  return SC_DD_OK;
+}
+
+uint64_t fnv_mix(uint64_t h, const void* p, size_t n) {
+  const unsigned char* c = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+  return h;
+}
+
+constexpr int kEngineGraphs = 8;
+
+// queue_batch through a CUDA graph when the same batch was queued before: the key covers the
+// inputs and strides, the drift plan, the threshold, the storage form, the process-wide
+// settings that change the launches, and the scratch generation.  Second sight: capture on
+// the engine's capture stream (ordered after `stream`) and launch; later: replay.  A batch
+// whose capture fails is queued directly from then on.
+int queue_batch_graphed(sc_dd* dd, int n, const float* const* inputs, const long long* strides, const DriftPlan& p,
+                        double snr_threshold, cudaStream_t stream, bool first_batch) {
+  uint64_t key = 1469598103934665603ull;
+  key = fnv_mix(key, &n, sizeof(n));
+  key = fnv_mix(key, inputs, sizeof(*inputs) * n);
+  key = fnv_mix(key, strides, sizeof(*strides) * n);
+  const int v[8] = {p.dmin, p.dmax, p.window_size, dd->precision, first_batch ? 1 : 0,
+                    scb::exact_statistics_always() ? 1 : 0, scb::stage_wait_tries(), (int)dd->generation};
+  key = fnv_mix(key, v, sizeof(v));
+  const long long stripe = scb::level_stripe_bytes();
+  key = fnv_mix(key, &stripe, sizeof(stripe));
+  key = fnv_mix(key, &snr_threshold, sizeof(snr_threshold));
+  cudaError_t e;
+  auto it = std::find_if(dd->graphs.begin(), dd->graphs.end(), [&](const sc_dd::Graph& g) { return g.key == key; });
+  if (it != dd->graphs.end()) {
+    it->last_use = ++dd->clock;
+    if ((e = cudaGraphLaunch(it->exec, stream)) != cudaSuccess) return cuda_fail(e, "graph launch");
+    return SC_DD_OK;
+  }
+  if (dd->seen.size() > 4096) dd->seen.clear();  // many different batches: forget old sightings
+  int& seen = dd->seen[key];
+  if (seen < 0 || ++seen < 2 || !dd->cap_stream) return queue_batch(dd, n, inputs, strides, p, snr_threshold, stream, first_batch);
+  if ((e = cudaEventRecord(dd->evj, stream)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(dd->cap_stream, dd->evj, 0)) != cudaSuccess)
+    return cuda_fail(e, "capture ordering");
+  if ((e = cudaStreamBeginCapture(dd->cap_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return cuda_fail(e, "begin capture");
+  const int rc = queue_batch(dd, n, inputs, strides, p, snr_threshold, dd->cap_stream, first_batch);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(dd->cap_stream, &g);
+  cudaGraphExec_t ex = nullptr;
+  if (rc == SC_DD_OK && e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (rc != SC_DD_OK || e != cudaSuccess || !ex) {
+    // not capturable: run it directly, now and from now on
+    cudaGetLastError();
+    seen = -1;
+    return queue_batch(dd, n, inputs, strides, p, snr_threshold, stream, first_batch);
+  }
+  if ((int)dd->graphs.size() >= kEngineGraphs) {
+    auto lru = std::min_element(dd->graphs.begin(), dd->graphs.end(),
+                                [](const sc_dd::Graph& a, const sc_dd::Graph& b) { return a.last_use < b.last_use; });
+    cudaGraphExecDestroy(lru->exec);
+    dd->graphs.erase(lru);
+  }
+  dd->graphs.push_back({key, ex, ++dd->clock});
+  if ((e = cudaGraphLaunch(ex, stream)) != cudaSuccess) return cuda_fail(e, "graph launch");
   return SC_DD_OK;
 }
 
@@ -346,7 +442,7 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
   long long d2h = 0;
   for (int k0 = 0; k0 < count; k0 += scb::kMaxBatch) {
     const int n = std::min(scb::kMaxBatch, count - k0);
-    rc = queue_batch(dd, n, inputs + k0, strides + k0, p, snr_threshold, stream, k0 == 0);
+    rc = queue_batch_graphed(dd, n, inputs + k0, strides + k0, p, snr_threshold, stream, k0 == 0);
     if (rc != SC_DD_OK) return rc;
     if (k0 == 0) cudaEventRecord(dd->ev[3], stream);
     // Headers of all n searches, then the first kHostCands candidates of each (strided copy).
@@ -427,8 +523,15 @@ int run_searches(sc_dd* dd, int count, const float* const* inputs, const long lo
     }
   }
   dd->last.d2h_bytes = (int)std::min<long long>(d2h, INT_MAX);
-  cudaEventElapsedTime(&dd->last.tree_ms, dd->ev[1], dd->ev[2]);
-  cudaEventElapsedTime(&dd->last.search_ms, dd->ev[0], dd->ev[3]);
+  // Timing is informational: a failed query leaves -1 and no pending error behind.
+  if (cudaEventElapsedTime(&dd->last.tree_ms, dd->ev[1], dd->ev[2]) != cudaSuccess) {
+    dd->last.tree_ms = -1.0f;
+    cudaGetLastError();
+  }
+  if (cudaEventElapsedTime(&dd->last.search_ms, dd->ev[0], dd->ev[3]) != cudaSuccess) {
+    dd->last.search_ms = -1.0f;
+    cudaGetLastError();
+  }
   dd->have_last = true;
   if (total > capacity) return fail(SC_DD_ETRUNC, "more hits than capacity");
   return SC_DD_OK;
@@ -495,6 +598,9 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
   }
   for (int i = 0; i < 4 && rc == SC_DD_OK; ++i)
     if ((e = cudaEventCreate(&d->ev[i])) != cudaSuccess) rc = cuda_fail(e, "sc_dd_create: event");
+  if (rc == SC_DD_OK && ((e = cudaStreamCreateWithFlags(&d->cap_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+                         (e = cudaEventCreateWithFlags(&d->evj, cudaEventDisableTiming)) != cudaSuccess))
+    rc = cuda_fail(e, "sc_dd_create: capture stream");
   if (rc != SC_DD_OK) {
     free_all(d);
     delete d;

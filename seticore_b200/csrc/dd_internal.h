@@ -318,6 +318,7 @@ struct LevelPlan {
 
 // L2 budget of one stripe pass of the one-level split (bytes; negative: the default).
 void set_level_stripe_bytes(long long bytes);
+long long level_stripe_bytes();  // the value set (negative: none)
 
 // Multi-level tree for Tr > 32 (one search): level kernels write the partial planes of
 // every sub-problem, then the fused max kernel finishes them (see dd_levels.cu).

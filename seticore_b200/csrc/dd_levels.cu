@@ -416,6 +416,7 @@ int default_first_level() {
 }  // namespace
 
 void set_level_stripe_bytes(long long bytes) { g_stripe_bytes.store(bytes < 0 ? -1 : bytes); }
+long long level_stripe_bytes() { return g_stripe_bytes.load(); }
 
 cudaError_t levels_search(const void* input_v, long long row_stride, int Tr, int N, int dmin, int dmax,
                           float* scratch_a, float* scratch_b, float* top, int num_sms,
