@@ -120,7 +120,14 @@ int sc_dd_search(sc_dd* dd, const float* dev_input, long long row_stride, int be
  * kernel, and the hits come back with one synchronisation per 64 searches.  Hits are
  * written search after search (each search's in increasing index order); num_hits[k]
  * receives search k's count.  The engine keeps scratch for the largest batch it has run
- * (the first call with a larger count, up to 64, allocates more). */
+ * (the first call with a larger count, up to 64, allocates more).
+ *
+ * Both calls keep CUDA graphs of repeated batches: a batch queued for the second time with the
+ * same input pointers and row strides, drift range, threshold, storage form and process-wide
+ * settings is captured (on a private stream ordered after `stream`) and later replayed on
+ * `stream`, which saves the per-kernel launch cost.  A replay reads the buffers' current
+ * contents; at most 8 graphs are kept, and growing the scratch drops them.  The calls
+ * synchronise `stream`, so they cannot themselves be captured into a caller's graph. */
 int sc_dd_search_batch(sc_dd* dd, int count, const float* const* dev_inputs,
                        const long long* row_strides, const int* beams,
                        const int* coarse_channels, double max_drift, double min_drift,
