@@ -107,6 +107,9 @@ struct sc_dd {
   scb::Candidate* cands = nullptr;
   float* scratch_a = nullptr;  // Tr > 32 level buffers (one search at a time), one allocation
   float* scratch_b = nullptr;  // = scratch_a + level_buffer_floats(Tr, N)
+  // The second pair (scratch_a + 2 and 3 level_buffer_floats, same allocation) with its
+  // stream and events: every other search of a batch runs its levels there.
+  scb::LevelSide side;
   void* host = nullptr;  // pinned: slots * (header + kHostCands candidates)
   int* inc_index = nullptr;
   int* inc_steps = nullptr;
@@ -238,7 +241,11 @@ void free_all(sc_dd* d) {
   free_slots(d);
   free_prec(d);
   d->scratch_b = nullptr;  // inside scratch_a's allocation
-  dfree(d, &d->scratch_a, 2 * sizeof(float) * scb::level_buffer_floats(d->Tr, d->N));
+  dfree(d, &d->scratch_a, 4 * sizeof(float) * scb::level_buffer_floats(d->Tr, d->N));
+  if (d->side.stream) cudaStreamDestroy(d->side.stream);
+  if (d->side.fork) cudaEventDestroy(d->side.fork);
+  if (d->side.join) cudaEventDestroy(d->side.join);
+  d->side = scb::LevelSide{};
   dfree(d, &d->inc_index, sizeof(int) * d->inc_cap);
   dfree(d, &d->inc_steps, sizeof(int) * d->inc_cap);
   dfree(d, &d->inc_vals, sizeof(float) * d->inc_cap);
@@ -354,7 +361,8 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
     if (h->record && cudaEventRecordWithFlags(h->dd->ev[2], st, cudaEventRecordExternal) != cudaSuccess)
       cudaGetLastError();
   };
-  cudaError_t e = scb::exec_queue(es, n, dd->scratch_a, dd->scratch_b, dd->num_sms, stream, hooks);
+  cudaError_t e = scb::exec_queue(es, n, dd->scratch_a, dd->scratch_b, dd->num_sms, stream, hooks,
+                                  dd->side.stream ? &dd->side : nullptr);
   if (e != cudaSuccess) return cuda_fail(e, "search kernels");
   return SC_DD_OK;
 }
@@ -589,12 +597,20 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
   // One slot; candidates for windows of 16 channels or more (grown when a call needs more).
   int rc = ensure_slots(d, 1, std::min(num_channels / 2 + 2, num_channels / 16 + 2));
   if (rc == SC_DD_OK && d->Tr > 32) {
-    // Both level buffers in one allocation: the emitting level addresses them as one array.
-    if ((e = dalloc(d, &d->scratch_a, 2 * sizeof(float) * scb::level_buffer_floats(d->Tr, num_channels))) !=
-        cudaSuccess)
+    // Both pairs of level buffers in one allocation: the emitting level addresses a pair as
+    // one array; the second pair serves the side stream.
+    const size_t L = scb::level_buffer_floats(d->Tr, num_channels);
+    if ((e = dalloc(d, &d->scratch_a, 4 * sizeof(float) * L)) != cudaSuccess) {
       rc = fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA, "sc_dd_create: level buffers");
-    else
-      d->scratch_b = d->scratch_a + scb::level_buffer_floats(d->Tr, num_channels);
+    } else {
+      d->scratch_b = d->scratch_a + L;
+      d->side.lvl_a = d->scratch_a + 2 * L;
+      d->side.lvl_b = d->scratch_a + 3 * L;
+      if ((e = cudaStreamCreateWithFlags(&d->side.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+          (e = cudaEventCreateWithFlags(&d->side.fork, cudaEventDisableTiming)) != cudaSuccess ||
+          (e = cudaEventCreateWithFlags(&d->side.join, cudaEventDisableTiming)) != cudaSuccess)
+        rc = cuda_fail(e, "sc_dd_create: level stream");
+    }
   }
   for (int i = 0; i < 4 && rc == SC_DD_OK; ++i)
     if ((e = cudaEventCreate(&d->ev[i])) != cudaSuccess) rc = cuda_fail(e, "sc_dd_create: event");

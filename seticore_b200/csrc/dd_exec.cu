@@ -117,7 +117,7 @@ TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride
 }  // namespace
 
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
-                       const ExecHooks& hooks) {
+                       const ExecHooks& hooks, const LevelSide* side) {
   cudaError_t e = cudaSuccess;
   for (int k0 = 0; k0 < n && e == cudaSuccess; k0 += kMaxBatch) {
     const int m = std::min(kMaxBatch, n - k0);
@@ -196,20 +196,40 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
           return e;
       }
     }
-    // More than 32 rows: the level path, one search at a time (shared level buffers); the
-    // 16-bit searches run it on their normalised copy, with the default split.
+    // More than 32 rows: the level path, one search at a time per level-buffer pair.  FP32
+    // searches alternate between the main stream and the side stream, when there is one (two
+    // concurrent 16-bit level searches measured slower than one after the other: their first
+    // level is bound by L1 throughput, not by latency); the 16-bit searches run it on their
+    // normalised copy, with the default split, on the main stream.
+    int n_level = 0;
+    for (int k = 0; k < m; ++k) n_level += ss[k].Tr > 32 && ss[k].elem == kElemF32;
+    const bool two = side && side->stream && n_level >= 2;
+    if (two) {
+      if ((e = cudaEventRecord(side->fork, stream)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(side->stream, side->fork, 0)) != cudaSuccess)
+        return e;
+    }
+    int j = 0;
     for (int k = 0; k < m; ++k) {
       if (ss[k].Tr <= 32) continue;
+      const bool on_side = two && ss[k].elem == kElemF32 && (j++ & 1);
+      cudaStream_t st = on_side ? side->stream : stream;
+      float* la = on_side ? side->lvl_a : lvl_a;
+      float* lb = on_side ? side->lvl_b : lvl_b;
       if (ss[k].elem != kElemF32) {
-        if ((e = levels_search(ss[k].norm16, ss[k].N, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
-                               ss[k].top16, num_sms, stream, LevelPlan{}, ss[k].elem, header_status(ss[k]))) !=
-            cudaSuccess)
+        if ((e = levels_search(ss[k].norm16, ss[k].N, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, la, lb, ss[k].top16,
+                               num_sms, st, LevelPlan{}, ss[k].elem, header_status(ss[k]))) != cudaSuccess)
           return e;
         continue;
       }
-      const LevelPlan plan = hooks.level_plan ? hooks.level_plan(hooks.ctx, ss[k], lvl_a, lvl_b, stream) : ss[k].level_plan;
-      if ((e = levels_search(ss[k].input, ss[k].row_stride, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, lvl_a, lvl_b,
-                             ss[k].top, num_sms, stream, plan, kElemF32, header_status(ss[k]))) != cudaSuccess)
+      const LevelPlan plan = hooks.level_plan ? hooks.level_plan(hooks.ctx, ss[k], la, lb, st) : ss[k].level_plan;
+      if ((e = levels_search(ss[k].input, ss[k].row_stride, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, la, lb,
+                             ss[k].top, num_sms, st, plan, kElemF32, header_status(ss[k]))) != cudaSuccess)
+        return e;
+    }
+    if (two) {
+      if ((e = cudaEventRecord(side->join, side->stream)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess)
         return e;
     }
     if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);

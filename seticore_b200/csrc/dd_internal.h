@@ -372,11 +372,24 @@ struct ExecHooks {
   void (*after_tree)(void* ctx, cudaStream_t s) = nullptr;
 };
 
+// A second stream with its own level buffers (the same size as the first pair, in one
+// allocation) and two events: exec_queue then runs every other search of more than 32 rows
+// on it, forked from and joined back into the main stream, so that the level kernels of two
+// searches share the SMs (they are bound by latency, with shared memory and registers the
+// respective limits).
+struct LevelSide {
+  cudaStream_t stream = nullptr;
+  float* lvl_a = nullptr;
+  float* lvl_b = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join = nullptr;
+};
+
 // Queues every kernel of n searches (any mix) on `stream`; no synchronisation.
 // lvl_a / lvl_b: level buffers of level_buffer_floats(Tr, N) floats for every search with
-// Tr > 32, in one allocation.
+// Tr > 32, in one allocation.  side: optional second stream for the level path.
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
-                       const ExecHooks& hooks);
+                       const ExecHooks& hooks, const LevelSide* side = nullptr);
 
 // Decodes a resolved candidate: returns false if the recovered path sum does not equal the
 // stored top sum (a consistency failure).  Paths are numbered (db - dmin) * Tr + off.

@@ -74,6 +74,7 @@ struct sc_dd_pool {
   float* lvl_a = nullptr;
   float* lvl_b = nullptr;
   size_t lvl_floats = 0;
+  scb::LevelSide side;  // its buffers: lvl_a + 2 and 3 lvl_floats, the same allocation
   char* host = nullptr;  // pinned: headers + candidate heads of the largest sub-batch
   size_t host_bytes = 0;
   cudaStream_t cap_stream = nullptr;
@@ -251,12 +252,15 @@ int ensure_device(sc_dd_pool* p, size_t arena, size_t lvl, cudaStream_t stream) 
   }
   if (lvl > p->lvl_floats) {
     if (p->lvl_a) cudaFreeAsync(p->lvl_a, stream);
-    p->lvl_a = p->lvl_b = nullptr;
+    p->lvl_a = p->lvl_b = p->side.lvl_a = p->side.lvl_b = nullptr;
     p->lvl_floats = 0;
-    // Both level buffers in one allocation: the emitting level addresses them as one array.
-    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&p->lvl_a), 2 * lvl * sizeof(float), stream)) != cudaSuccess)
+    // Both pairs of level buffers in one allocation: the emitting level addresses a pair as
+    // one array; the second pair serves the side stream.
+    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&p->lvl_a), 4 * lvl * sizeof(float), stream)) != cudaSuccess)
       return pfail(SC_DD_ENOMEM, std::string("pool level buffers: ") + cudaGetErrorString(e));
     p->lvl_b = p->lvl_a + lvl;
+    p->side.lvl_a = p->lvl_a + 2 * lvl;
+    p->side.lvl_b = p->lvl_a + 3 * lvl;
     p->lvl_floats = lvl;
   }
   return SC_DD_OK;
@@ -270,7 +274,9 @@ cudaError_t queue_sub(sc_dd_pool* p, std::vector<Planned>& sub, cudaStream_t s) 
   hooks.ctx = p;
   hooks.tree_launch = pool_tree_launch;
   hooks.level_plan = pool_level_plan;
-  cudaError_t e = scb::exec_queue(es.data(), (int)es.size(), p->lvl_a, p->lvl_b, p->num_sms, s, hooks);
+  // The tuner times one level search at a time on its own stream: no side stream then.
+  cudaError_t e = scb::exec_queue(es.data(), (int)es.size(), p->lvl_a, p->lvl_b, p->num_sms, s, hooks,
+                                  p->tuning_now ? nullptr : &p->side);
   if (e != cudaSuccess) return e;
   char* h = p->host;
   for (size_t k = 0; k < sub.size(); ++k) {
@@ -300,6 +306,9 @@ int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out) {
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->side.join, cudaEventDisableTiming);
   for (cudaEvent_t* ev : {&p->ev0, &p->ev1, &p->evj, &p->t0, &p->t1})
     if (e == cudaSuccess) e = cudaEventCreate(ev);
   // The host buffer of the largest possible sub-batch, allocated once: pinned allocations
@@ -308,6 +317,10 @@ int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out) {
   if (e == cudaSuccess) e = cudaMallocHost(&p->host, p->host_bytes);
   if (e != cudaSuccess) {
     if (p->host) cudaFreeHost(p->host);
+    for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1, p->side.fork, p->side.join})
+      if (ev) cudaEventDestroy(ev);
+    for (cudaStream_t st : {p->cap_stream, p->side.stream})
+      if (st) cudaStreamDestroy(st);
     delete p;
     return pcuda(e, "sc_dd_pool_create");
   }
@@ -328,6 +341,9 @@ int sc_dd_pool_destroy(sc_dd_pool* p) {
   for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1})
     if (ev) cudaEventDestroy(ev);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  if (p->side.stream) cudaStreamDestroy(p->side.stream);
+  for (cudaEvent_t ev : {p->side.fork, p->side.join})
+    if (ev) cudaEventDestroy(ev);
   delete p;
   return SC_DD_OK;
 }
