@@ -24,14 +24,21 @@ import numpy as np
 from .pool import SearchPool, SearchRequest
 
 
-def admit(pending_bytes, free_bytes: int, max_batch: int) -> int:
+def admit(pending_bytes, free_bytes: int, max_batch: int, pending_samples=None, max_samples=None) -> int:
     """How many of the pending requests (in arrival order) the next batch takes: the
-    longest prefix whose bytes fit the free budget, at most max_batch."""
+    longest prefix whose bytes fit the free budget, at most max_batch, and -- when
+    max_samples is given -- whose samples (timesteps x channels) stay within max_samples,
+    though the first request is always taken if it fits the budget."""
     n = 0
-    for b in pending_bytes:
+    work = 0
+    for i, b in enumerate(pending_bytes):
         if n >= max_batch or b > free_bytes:
             break
+        if max_samples is not None and n > 0 and work + pending_samples[i] > max_samples:
+            break
         free_bytes -= b
+        if max_samples is not None:
+            work += pending_samples[i]
         n += 1
     return n
 
@@ -41,16 +48,18 @@ class _Pending:
     req: SearchRequest
     bytes: int
     arrival: float
+    samples: int = 0
     future: Future = field(default_factory=Future)
 
 
 class SearchServer:
     def __init__(self, hbm_budget_bytes: int = 120 << 30, workers: int = 2, max_batch: int = 64,
-                 input_bytes=None):
+                 input_bytes=None, max_batch_samples: Optional[int] = None):
         import torch
         self.budget = int(hbm_budget_bytes)
         self.used = 0
         self.max_batch = max_batch
+        self.max_batch_samples = max_batch_samples
         self._input_bytes = input_bytes or (lambda r: r.input.numel() * r.input.element_size())
         self._q: deque = deque()
         self._cv = threading.Condition()
@@ -67,7 +76,7 @@ class SearchServer:
 
     def submit(self, req: SearchRequest) -> Future:
         cost = self._input_bytes(req) + SearchPool.scratch_bytes(req)
-        p = _Pending(req, cost, time.perf_counter())
+        p = _Pending(req, cost, time.perf_counter(), int(req.input.shape[0]) * int(req.input.shape[1]))
         if cost > self.budget:
             p.future.set_exception(MemoryError(f"request needs {cost} bytes, budget is {self.budget}"))
             return p.future
@@ -93,8 +102,10 @@ class SearchServer:
                 p.configure(self._autotune)
 
     def _take(self) -> List[_Pending]:
-        """Pending requests, in arrival order, that fit the free budget (at most max_batch)."""
-        n = admit([p.bytes for p in self._q], self.budget - self.used, self.max_batch)
+        """Pending requests, in arrival order, that fit the free budget (at most max_batch
+        requests and max_batch_samples samples)."""
+        n = admit([p.bytes for p in self._q], self.budget - self.used, self.max_batch,
+                  [p.samples for p in self._q], self.max_batch_samples)
         return [self._q.popleft() for _ in range(n)]
 
     def _work(self, stream):

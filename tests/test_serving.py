@@ -12,6 +12,10 @@ def test_admission_takes_the_fitting_prefix():
     assert admit([50, 10], 40, 64) == 0          # in order: a large head blocks (no reordering)
     assert admit([1] * 100, 1000, 64) == 64      # batch cap
     assert admit([], 100, 64) == 0
+    # a sample cap bounds a batch's work, but the head request is always taken
+    assert admit([1, 1, 1], 100, 64, [40, 40, 40], 100) == 2
+    assert admit([1, 1], 100, 64, [500, 10], 100) == 1
+    assert admit([1, 1], 100, 64, [10, 10], None) == 2
 
 
 @pytest.mark.gpu
