@@ -141,11 +141,12 @@ def bytes_fused_fp32(Tr, n):
     return 4 * Tr * n + 8 * n
 
 
-def bytes_fused_16bit(Tr, n):
-    """What the 16-bit forms must move per search: the float32 input read once by the
-    normalising pass (plus three sampled rows for its scale), the 16-bit copy written and read
-    once by the tree, and the per-channel tops and column sums: 4*Tr*N + 12*N + 2*Tr*N*2 + 8*N."""
-    return 8 * Tr * n + 20 * n
+def bytes_paired_16bit(Tr, n):
+    """What the 16-bit forms of a 16-row search must move, their tree adding FP16 pairs of two
+    drift blocks: the float32 input read once by the normalising pass (plus three sampled rows
+    for its scale), the paired copy (4 bytes per value) written and read once by the tree, and
+    the per-channel tops and column sums: 4*Tr*N + 12*N + 4*Tr*N*2 + 8*N."""
+    return 12 * Tr * n + 20 * n
 
 
 def num_sms():
@@ -550,13 +551,14 @@ def main():
         barrier(world)
         st = dd.last_stats()
         p_ms = max_over_ranks(p0.elapsed_time(p1) / args.steps, world)
-        alg16 = bytes_fused_16bit(T, N) * n_coarse
+        alg16 = bytes_paired_16bit(T, N) * n_coarse
         peak16, _ = measured_peak_hbm()
         precision[prec] = {"value": world * samples_per_step / (p_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": p_ms,
                            "hbm_frac_of_step": alg16 / (p_ms / 1e3) / 1e9 / peak16,
                            "bytes_per_step": alg16,
-                           "bytes_per_step_note": "three sampled rows + one normalising read/write + one 16-bit "
-                                                  "tree read + tops and column sums (8*Tr*N + 20*N per search)",
+                           "bytes_per_step_note": "three sampled rows + one normalising read, the paired FP16 "
+                                                  "copy written and read once by the tree, tops and column sums "
+                                                  "(12*Tr*N + 20*N per search)",
                            "hits_identical_to_fp32": identical,
                            "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}",
                            "speedup_vs_fp32": ms / p_ms}

@@ -191,6 +191,14 @@ int sc_dd_set_level_stripe_bytes(long long bytes);
  * CUDA graph keeps the mode it was captured with).  Other modes: SC_DD_EINVAL. */
 int sc_dd_set_exact_statistics(int mode);
 
+/* No counterpart in the reference (which has no 16-bit form).  on 1 (the default): the BF16
+ * and FP16 forms' searches of 16 rounded timesteps run their approximate tree in FP16 pairs,
+ * two drift blocks per instruction; the flag bound then covers FP16 adds, so a few more
+ * channels are recomputed in float32.  on 0: that tree accumulates in float32.  The hit
+ * lists are identical either way.  Process-wide; launches queued after the call follow it (a
+ * CUDA graph keeps the form it was captured with).  Other values: SC_DD_EINVAL. */
+int sc_dd_set_paired_fp16(int on);
+
 /* The device half of H5Reader::loadCoarseChannel (h5_reader.cpp:190-209) for `count`
  * coarse channels laid out item_stride floats apart, each [rounded_timesteps][row_stride]:
  * rows num_timesteps .. rounded_timesteps-1 become zero and, if has_dc_spike, column

@@ -35,6 +35,7 @@ EXPORTED = [
     "sc_dd_prepare_coarse_channels", "sc_dd_gather_columns", "sc_dd_set_stage_wait_limit",
     "sc_dd_set_level_stripe_bytes",
     "sc_dd_set_exact_statistics",
+    "sc_dd_set_paired_fp16",
 ]
 
 
@@ -152,6 +153,7 @@ def lib():
         L.sc_dd_set_stage_wait_limit.argtypes = [i]
         L.sc_dd_set_level_stripe_bytes.argtypes = [ctypes.c_longlong]
         L.sc_dd_set_exact_statistics.argtypes = [i]
+        L.sc_dd_set_paired_fp16.argtypes = [i]
         L.sc_dd_last_error.restype = ctypes.c_char_p
         L.sc_dd_version.restype = ctypes.c_char_p
         for name in EXPORTED:

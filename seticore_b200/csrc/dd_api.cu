@@ -118,7 +118,7 @@ struct sc_dd {
   // Precision form (16-bit normalised storage), per slot.
   int precision = SC_DD_PRECISION_FP32;
   int prec_slots = 0;
-  void* norm16 = nullptr;        // [slot][Tr][N] 16-bit
+  void* norm16 = nullptr;        // [slot] normalised copies of norm_buffer_bytes(Tr, N)
   float* top16 = nullptr;        // [slot][N]
   int* flags = nullptr;          // [slot][N] flagged channels
   int* flag_counts = nullptr;    // [slot]
@@ -194,7 +194,7 @@ void free_slots(sc_dd* d) {
 
 void free_prec(sc_dd* d) {
   const size_t S = d->prec_slots, N = d->N;
-  dfree(d, &d->norm16, 2 * N * d->Tr * S);
+  dfree(d, &d->norm16, scb::norm_buffer_bytes(d->Tr, (int)N) * S);
   dfree(d, &d->top16, sizeof(float) * N * S);
   dfree(d, &d->flags, sizeof(int) * N * S);
   dfree(d, &d->flag_counts, sizeof(int) * S);
@@ -214,7 +214,7 @@ int ensure_prec(sc_dd* d, int slots) {
   free_prec(d);
   const size_t S = slots, N = d->N;
   cudaError_t e;
-  if ((e = dalloc(d, &d->norm16, 2 * N * d->Tr * S)) != cudaSuccess ||
+  if ((e = dalloc(d, &d->norm16, scb::norm_buffer_bytes(d->Tr, (int)N) * S)) != cudaSuccess ||
       (e = dalloc(d, &d->top16, sizeof(float) * N * S)) != cudaSuccess ||
       (e = dalloc(d, &d->flags, sizeof(int) * N * S)) != cudaSuccess ||
       (e = dalloc(d, &d->flag_counts, sizeof(int) * S)) != cudaSuccess ||
@@ -338,7 +338,7 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
     q.hdr = dd->hdrs + k;
     q.cands = dd->cands + (size_t)dd->cand_cap * k;
     if (prec) {
-      q.norm16 = static_cast<char*>(dd->norm16) + (size_t)2 * dd->N * dd->Tr * k;
+      q.norm16 = static_cast<char*>(dd->norm16) + scb::norm_buffer_bytes(dd->Tr, dd->N) * k;
       q.top16 = dd->top16 + N * k;
       q.flags = dd->flags + N * k;
       q.flag_count = dd->flag_counts + k;
@@ -386,8 +386,9 @@ int queue_batch_graphed(sc_dd* dd, int n, const float* const* inputs, const long
   key = fnv_mix(key, &n, sizeof(n));
   key = fnv_mix(key, inputs, sizeof(*inputs) * n);
   key = fnv_mix(key, strides, sizeof(*strides) * n);
-  const int v[8] = {p.dmin, p.dmax, p.window_size, dd->precision, first_batch ? 1 : 0,
-                    scb::exact_statistics_always() ? 1 : 0, scb::stage_wait_tries(), (int)dd->generation};
+  const int v[9] = {p.dmin, p.dmax, p.window_size, dd->precision, first_batch ? 1 : 0,
+                    scb::exact_statistics_always() ? 1 : 0, scb::stage_wait_tries(), (int)dd->generation,
+                    scb::paired_fp16() ? 1 : 0};
   key = fnv_mix(key, v, sizeof(v));
   const long long stripe = scb::level_stripe_bytes();
   key = fnv_mix(key, &stripe, sizeof(stripe));
@@ -566,6 +567,12 @@ int sc_dd_set_level_stripe_bytes(long long bytes) {
 int sc_dd_set_exact_statistics(int mode) {
   if (mode != 0 && mode != 1) return fail(SC_DD_EINVAL, "sc_dd_set_exact_statistics: mode must be 0 or 1");
   scb::set_exact_statistics_always(mode == 1);
+  return SC_DD_OK;
+}
+
+int sc_dd_set_paired_fp16(int on) {
+  if (on != 0 && on != 1) return fail(SC_DD_EINVAL, "sc_dd_set_paired_fp16: on must be 0 or 1");
+  scb::set_paired_fp16(on == 1);
   return SC_DD_OK;
 }
 

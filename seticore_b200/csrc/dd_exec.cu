@@ -62,7 +62,10 @@ SearchDesc to_desc(const ExecSearch& e) {
   return s;
 }
 
-PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
+// 16-bit 16-row searches take the paired-FP16 tree when it is on (the flag bound must know).
+bool pair16_search(const ExecSearch& e, bool on) { return on && e.elem != kElemF32 && e.Tr == 16; }
+
+PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr, bool pair_on) {
   PrecisionDesc q{};
   q.input = e.input;
   q.row_stride = e.row_stride;
@@ -81,6 +84,7 @@ PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr) {
   q.top = e.top;
   q.flag_list = e.flags;
   q.flag_count = e.flag_count;
+  q.pair16 = pair16_search(e, pair_on) ? 1 : 0;
   return q;
 }
 
@@ -119,6 +123,7 @@ TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
                        const ExecHooks& hooks, const LevelSide* side) {
   cudaError_t e = cudaSuccess;
+  const bool pair_on = paired_fp16();  // read once: the trees and the flag bounds agree
   for (int k0 = 0; k0 < n && e == cudaSuccess; k0 += kMaxBatch) {
     const int m = std::min(kMaxBatch, n - k0);
     const ExecSearch* ss = s + k0;
@@ -136,7 +141,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
     clear_pb.elem = kElemBF16;
     for (int k = 0; k < m; ++k) {
       clear_pb.s[k] = PrecisionDesc{};
-      if (ss[k].elem != kElemF32) clear_pb.s[k] = to_pdesc(ss[k], b.s[k].hdr);
+      if (ss[k].elem != kElemF32) clear_pb.s[k] = to_pdesc(ss[k], b.s[k].hdr, pair_on);
     }
     {
       int gx = (b.maxN + 1023) / 1024;
@@ -152,7 +157,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       q.elem = elem;
       for (int k = 0; k < m; ++k)
         if (ss[k].elem == elem) {
-          q.s[q.count++] = to_pdesc(ss[k], b.s[k].hdr);
+          q.s[q.count++] = to_pdesc(ss[k], b.s[k].hdr, pair_on);
           q.maxN = std::max(q.maxN, ss[k].N);
         }
       if (q.count && (e = normalize_batch(q, num_sms, stream)) != cudaSuccess) return e;
@@ -178,6 +183,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
         TreeBatch tb;
         tb.count = 0;
         tb.n_items = 0;
+        tb.pair16 = (elem != kElemF32 && R == 16 && pair_on) ? 1 : 0;
         for (int k = 0; k < m; ++k) {
           if (ss[k].Tr != R || ss[k].elem != elem) continue;
           if (elem == kElemF32) {
@@ -186,6 +192,12 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
               g.colsum = ss[k].colsum;
               g.colsum_job = -ss[k].dmin;
             }
+            tb.g[tb.count++] = g;
+          } else if (tb.pair16) {
+            // the paired copy: channel 0 of row 0 sits kPairPad words into the buffer
+            TreeGroup g = tree_group(ss[k], static_cast<const uint32_t*>(ss[k].norm16) + kPairPad,
+                                     pair_row_words(ss[k].N), ss[k].top16);
+            g.pad = kPairPad;
             tb.g[tb.count++] = g;
           } else {
             tb.g[tb.count++] = tree_group(ss[k], ss[k].norm16, ss[k].N, ss[k].top16);
@@ -243,7 +255,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       q.elem = kElemBF16;
       for (int k = 0; k < m; ++k)
         if (ss[k].elem != kElemF32) {
-          q.s[q.count++] = to_pdesc(ss[k], b.s[k].hdr);
+          q.s[q.count++] = to_pdesc(ss[k], b.s[k].hdr, pair_on);
           q.maxN = std::max(q.maxN, ss[k].N);
         }
       if (q.count) {
@@ -262,7 +274,7 @@ size_t ExecSearch::scratch_bytes(int Tr, int N, int cand_cap, int n_partials, in
              a(sizeof(double) * 2 * kVarChunks) + a(sizeof(float) * order_work_floats(N)) +
              a(sizeof(int) * order_list_entries(N)) + a(sizeof(SearchHeader)) + a(sizeof(Candidate) * cand_cap);
   if (elem != kElemF32) {
-    b += a((size_t)2 * Tr * N) + a(sizeof(float) * N) + a(sizeof(int) * N) + a(sizeof(int)) +
+    b += a(norm_buffer_bytes(Tr, N)) + a(sizeof(float) * N) + a(sizeof(int) * N) + a(sizeof(int)) +
          a(sizeof(double) * kNormMomentsDoubles) + a(sizeof(unsigned));
   }
   return b;
@@ -291,7 +303,7 @@ void ExecSearch::carve(char* base, int n_partials) {
   p += a(sizeof(Candidate) * cand_cap);
   if (elem != kElemF32) {
     norm16 = p;
-    p += a((size_t)2 * Tr * N);
+    p += a(norm_buffer_bytes(Tr, N));
     top16 = reinterpret_cast<float*>(p);
     p += a(sizeof(float) * N);
     flags = reinterpret_cast<int*>(p);

@@ -160,6 +160,9 @@ struct TreeGroup {
   int item_begin;  // first work item of this group in the launch
   // Optional: set to 1 if a staging wait of the tree gave up (its results are then invalid).
   int* status;
+  // Elements before channel 0 that the rows hold (read as data, not as zeros): kPairPad for
+  // the paired-FP16 copy, 0 otherwise.
+  int pad;
 };
 
 struct TreeBatch {
@@ -171,8 +174,16 @@ struct TreeBatch {
   // L2 hints of the bulk copies: 0 none; 1 (stripe passes' first level) staged input rows
   // evict-first and emitted planes evict-last, so the planes stay in L2 for the last level.
   int cache_mode = 0;
+  // 1: the groups are 16-bit rows of 16-row searches, run by the paired-FP16 tree (two drift
+  // blocks per unit, FP16 sums; the precision form's flag bound then takes FP16 adds).
+  int pair16 = 0;
   TreeGroup g[kMaxBatch];
 };
+
+// Whether 16-bit 16-row searches queued from now on take the paired-FP16 tree (default on;
+// off: the float-accumulating 16-bit tree).  The hit lists are the same either way.
+void set_paired_fp16(bool on);
+bool paired_fp16();
 
 // The staging-wait poll limit of tree launches queued from now on (negative: the default).
 // Tests set 0 to make every staged item give up, which exercises the give-up path (the
@@ -216,6 +227,19 @@ inline long long level_row_length(int N) {
 // four drift blocks of a last level of up to 16 rows, dd_levels.cu), so the two level
 // buffers hold a whole-row pass of two drift blocks.
 constexpr long long kLevelRowSlack = 2048;
+// The paired-FP16 copy of a 16-row search (the 16-bit forms' paired tree): row t holds, for
+// channel x in [-kPairPad, N), the word (y[t][x], y[t][x + t]) as two FP16 values (0 outside
+// [0, N)), kPairPad words before channel 0 and rows pair_row_words(N) words apart.
+constexpr int kPairPad = 16;
+inline long long pair_row_words(int N) { return ((long long)N + kPairPad + 3) / 4 * 4; }
+// Bytes of a search's normalised copy: the dense 16-bit [Tr][N] copy, or for 16 rows room
+// for the paired copy as well (whichever the paired-FP16 setting picks at launch).
+inline size_t norm_buffer_bytes(int Tr, int N) {
+  const size_t dense = (size_t)2 * Tr * N;
+  const size_t paired = Tr == 16 ? (size_t)4 * Tr * (size_t)pair_row_words(N) : 0;
+  return dense > paired ? dense : paired;
+}
+
 inline size_t level_buffer_floats(int Tr, int N) {
   return (size_t)Tr * (size_t)(level_row_length(N) + kLevelRowSlack);
 }
@@ -236,6 +260,8 @@ struct PrecisionDesc {
   float* top;           // exact float32 tops of the flagged channels (others stay 0)
   int* flag_list;       // flagged channels (capacity N)
   int* flag_count;
+  int pair16;           // 1: norm holds the paired-FP16 copy and the tops come from the
+                        // paired-FP16 tree (FP16 adds)
 };
 struct PrecisionBatch {
   int count;

@@ -115,7 +115,7 @@ scb::TreeLaunch pool_tree_launch(void* ctx, const scb::TreeBatch& tb, int R, int
     max_jobs = std::max(max_jobs, tb.g[k].n_jobs);
     channels += tb.g[k].N;
   }
-  const int v[4] = {R, elem, bucket(max_jobs), bucket(channels)};
+  const int v[5] = {R, elem, bucket(max_jobs), bucket(channels), tb.pair16};
   const uint64_t key = fnv(1469598103934665603ull, v, sizeof(v));
   auto it = p->tuned_launch.find(key);
   if (it != p->tuned_launch.end()) return it->second;
@@ -454,6 +454,10 @@ int sc_dd_pool_search(sc_dd_pool* p, const sc_dd_request* reqs, int count, sc_dd
       const sc_dd_request& r = reqs[sb.first + (&pl - sub.data())];
       key = fnv(key, &r, sizeof(r));
     }
+    // and the process-wide settings that change the launches
+    const long long settings[4] = {scb::exact_statistics_always() ? 1 : 0, scb::stage_wait_tries(),
+                                   scb::paired_fp16() ? 1 : 0, scb::level_stripe_bytes()};
+    key = fnv(key, settings, sizeof(settings));
     p->st.sub_batches++;
     auto git = std::find_if(p->graphs.begin(), p->graphs.end(), [&](const sc_dd_pool::Graph& g) { return g.key == key; });
     if (p->use_graphs && git != p->graphs.end()) {

@@ -6,9 +6,10 @@
 //      FP64, rounded to BF16 or FP16 (padded rows stay 0), into a dense [Tr][N] 16-bit copy
 //      -- half the bytes of the input -- and, in the same read, the float32 column sums the
 //      statistics need and the minimum and maximum of the unrounded rows.
-//   3. (dd_tree.cu, dd_levels.cu) the tree over y, accumulating in FP32, gives approximate
-//      tops.  A path sum of y equals (P - T*mean) / std for the path sum P of x, so the
-//      order of path sums is kept up to the 16-bit rounding.
+//   3. (dd_tree.cu, dd_levels.cu) the tree over y, accumulating in FP32 (or, for 16 rows,
+//      in FP16 pairs: two drift blocks per instruction), gives approximate tops.  A path
+//      sum of y equals (P - T*mean) / std for the path sum P of x, so the order of path sums
+//      is kept up to the rounding.
 //   4. flag_channels_kernel: lists every channel whose approximate top reaches the flag
 //      threshold, the threshold mapped to y units less a bound on the rounding of the
 //      16-bit values and of both float trees (flag_threshold).
@@ -28,6 +29,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "dd_common.cuh"
 #include "dd_internal.h"
@@ -232,6 +234,132 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
   d.moments[2 * kVarChunks + 3] = omx;
 }
 
+// The normalised value y as the FP16 bits the paired tree adds: rounded to the storage form
+// first (BF16 values are then exact in FP16 within its normal range, and at most 2^-25 off
+// below it).
+template <typename E>
+__device__ __forceinline__ unsigned short pair_bits(float y) {
+  if constexpr (std::is_same<E, __half>::value) {
+    return __half_as_ushort(__float2half_rn(y));
+  } else {
+    return __half_as_ushort(__float2half_rn(__bfloat162float(__float2bfloat16_rn(y))));
+  }
+}
+
+// The paired copy of a 16-row search (the paired-FP16 tree's input): the same single read as
+// normalize_kernel -- y in FP64, rounded to the storage form, the float32 column sums in row
+// order and the extremes -- but it writes, for row t and channel x in [-kPairPad, N), the word
+// (y[t][x], y[t][x + t]) as two FP16 values (0 outside [0, N)): the leaves of drift blocks k
+// and k + 1 side by side, since the tree reads row t of drift block k + 1 t channels further.
+// A block takes kPairCols channels at a time, four per thread (256 threads): their values,
+// and those of the next kPairPad channels, go to shared memory, then every word of its
+// channels is written whole (16-byte stores).
+constexpr int kPairCols = 1024;
+template <typename E>
+__global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_constant__ PrecisionBatch b) {
+  const PrecisionDesc& d = b.s[blockIdx.y];
+  // rows of kPairCols + kPairPad values; 2080 bytes, so every 4-value group is 8-byte aligned
+  __shared__ __align__(16) unsigned short ys[16][kPairCols + kPairPad];
+  const double mean = d.moments[2 * kVarChunks];
+  const double inv = 1.0 / d.moments[2 * kVarChunks + 1];
+  uint32_t* out = static_cast<uint32_t*>(d.norm);
+  const long long np = ((long long)d.N + kPairPad + 3) / 4 * 4;  // pair_row_words(N)
+  const int N = d.N, T = d.T;
+  float mn = __int_as_float(0x7f800000), mx = -mn;  // NaNs are skipped (they flag themselves)
+  const bool vec = (N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
+  for (long long c0 = (long long)blockIdx.x * kPairCols; c0 < N; c0 += (long long)gridDim.x * kPairCols) {
+    // the next kPairPad channels' values (the second elements of the last words): one value
+    // per thread, issued before the block's own loads
+    {
+      const int t = threadIdx.x >> 4, i = threadIdx.x & 15;
+      const long long x = c0 + kPairCols + i;
+      unsigned short h = 0;
+      if (x < N && t < T) h = pair_bits<E>((float)(((double)__ldg(d.input + (long long)t * d.row_stride + x) - mean) * inv));
+      ys[t][kPairCols + i] = h;
+    }
+    // four channels per thread down the 16 rows, eight rows' loads in flight at a time;
+    // channels past N are 0 and do not enter the sums or the extremes
+    const long long c = c0 + 4 * threadIdx.x;
+    const bool full = vec && c + 3 < N;
+    const int nin = c >= N ? 0 : (c + 3 < N ? 4 : (int)(N - c));
+    float cs[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int g = 0; g < 16; g += 8) {
+      float e[8][4];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const float* row = d.input + (long long)(g + u) * d.row_stride;
+        if (full) {
+          const float4 q = __ldg(reinterpret_cast<const float4*>(row + c));
+          e[u][0] = q.x;
+          e[u][1] = q.y;
+          e[u][2] = q.z;
+          e[u][3] = q.w;
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) e[u][i] = i < nin ? __ldg(row + c + i) : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int t = g + u;
+        unsigned long long packed = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) cs[i] += e[u][i];
+        if (t < T) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (i < nin) {
+              packed |= (unsigned long long)pair_bits<E>((float)(((double)e[u][i] - mean) * inv)) << (16 * i);
+              mn = fminf(mn, e[u][i]);
+              mx = fmaxf(mx, e[u][i]);
+            }
+          }
+        }
+        *reinterpret_cast<unsigned long long*>(&ys[t][4 * threadIdx.x]) = packed;
+      }
+    }
+    if (d.colsum) {
+      if (nin == 4) {
+        reinterpret_cast<float4*>(d.colsum + c)[0] = make_float4(cs[0], cs[1], cs[2], cs[3]);
+      } else {
+        for (int i = 0; i < nin; ++i) d.colsum[c + i] = cs[i];
+      }
+    }
+    __syncthreads();
+    // words (y[t][j], y[t][j + t]): the second values are the four starting t further, taken
+    // from two aligned 8-byte loads by a constant shift (t is unrolled)
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const unsigned long long lo = *reinterpret_cast<const unsigned long long*>(&ys[t][4 * threadIdx.x]);
+      const unsigned long long ha = *reinterpret_cast<const unsigned long long*>(&ys[t][4 * threadIdx.x + (t & ~3)]);
+      const unsigned long long hb = *reinterpret_cast<const unsigned long long*>(&ys[t][4 * threadIdx.x + (t & ~3) + 4]);
+      const unsigned long long hi = (t & 3) ? (ha >> (16 * (t & 3))) | (hb << (64 - 16 * (t & 3))) : ha;
+      const uint32_t l0 = (uint32_t)lo, l1 = (uint32_t)(lo >> 32), h0 = (uint32_t)hi, h1 = (uint32_t)(hi >> 32);
+      const uint4 w = make_uint4(__byte_perm(l0, h0, 0x5410), __byte_perm(l0, h0, 0x7632), __byte_perm(l1, h1, 0x5410),
+                                 __byte_perm(l1, h1, 0x7632));
+      uint32_t* dst = out + (long long)t * np + kPairPad + c;
+      if (nin == 4) {
+        *reinterpret_cast<uint4*>(dst) = w;
+      } else {
+        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+        for (int i = 0; i < nin; ++i) dst[i] = ws[i];
+      }
+    }
+    // the kPairPad words before channel 0: (0, y[t][x + t])
+    if (c0 == 0 && threadIdx.x < 16) {
+      const int t = threadIdx.x;
+      for (int x = -kPairPad; x < 0; ++x)
+        out[(long long)t * np + kPairPad + x] = x + t >= 0 ? (uint32_t)ys[t][x + t] << 16 : 0u;
+    }
+    __syncthreads();
+  }
+  double a, q, omn, omx;
+  if (!fold_moments(d, 0.0, 0.0, mn, mx, &a, &q, &omn, &omx)) return;
+  d.moments[2 * kVarChunks + 2] = omn;
+  d.moments[2 * kVarChunks + 3] = omx;
+}
+
 // The flag threshold in normalised path-sum units: every channel whose float32 top P_f
 // (the plain form's, tree order) reaches the search's threshold `thr` has an approximate
 // top S~ (the 16-bit tree's) of at least this value, so it is listed and recomputed.
@@ -248,6 +376,13 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
 // If P_f >= thr then P >= a_x := thr - g (|thr| + 2 T Xn) (1 + 2g), i.e. S_y >= a =
 // (a_x - T mean) / std, and S~ >= S_y - c (|S_y| + 2 T Ym) - T e_abs with c = u + g (1 + u).
 // The right side grows with S_y (c < 1), so its value at S_y = a bounds S~ from below.
+//
+// The paired-FP16 tree (pair16) adds in FP16 instead: each add is off by at most 2^-11 of
+// its result or, below FP16's normal range, by 2^-25 absolute, so its sums are within
+// h sum|terms| + Tr 2^-25 (1.01) with h = 1.01 L 2^-11; BF16 leaves are rounded to FP16 on the
+// way (e_abs = 2^-25 for both forms).  Then S~ >= S_y - c (|S_y| + 2 T Ym) - T e_abs (1 + h)
+// - 1.01 Tr 2^-25 with c = u + h (1 + u).  No partial sum can overflow while Tr * ymax
+// stays below 60000 (FP16's largest value is 65504); beyond it every channel is listed.
 // A margin of 2^-20 relative guards the double arithmetic here; NaN inputs and NaN tops are
 // always listed.
 __device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem) {
@@ -257,19 +392,23 @@ __device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem
   const int L = 31 - __clz(d.Tr);
   const double g = 1.01 * L * 0x1p-24;
   const bool fp16 = (elem == kElemF16);
+  const bool pair = d.pair16 != 0;
+  const double h = pair ? 1.01 * L * 0x1p-11 : g;  // the 16-bit tree's own add bound
   const double u = (fp16 ? 0x1p-11 : 0x1p-8) + 0x1p-24;
-  const double e_abs = fp16 ? 0x1p-25 : 0.0;
+  const double e_abs = (fp16 || pair) ? 0x1p-25 : 0.0;
   const double T = (double)d.T;
   const double xn = xmin < 0.0 ? -xmin : 0.0;
   const double ym = fmax(0.0, (mean - xmin) / sd);
   const double a_x = thr - g * (fabs(thr) + 2.0 * T * xn) * (1.0 + 2.0 * g);
   const double a = (a_x - T * mean) / sd;
-  const double c = u + g * (1.0 + u);
-  const double lo = a - c * (fabs(a) + 2.0 * T * ym) - T * e_abs;
-  // Normalised values beyond the 16-bit range (a scale from an unrepresentative sample)
-  // void the relative bounds: then every channel is listed.
+  const double c = u + h * (1.0 + u);
+  const double sub = pair ? 1.01 * (double)d.Tr * 0x1p-25 : 0.0;
+  const double lo = a - c * (fabs(a) + 2.0 * T * ym) - T * e_abs * (1.0 + h) - sub;
+  // Normalised values beyond the 16-bit range (a scale from an unrepresentative sample), or
+  // paired-FP16 sums that could overflow, void the bounds: then every channel is listed.
   const double ymax = fmax(fabs(xmax - mean), fabs(xmin - mean)) / sd;
-  if (!(ymax < (fp16 ? 60000.0 : 1e38))) return __int_as_float(0xff800000);  // -inf
+  const double ylim = pair ? 60000.0 / (double)d.Tr : (fp16 ? 60000.0 : 1e38);
+  if (!(ymax < ylim)) return __int_as_float(0xff800000);  // -inf
   return (float)(lo - 0x1p-20 * (fabs(lo) + 1.0));
 }
 
@@ -368,8 +507,23 @@ cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
   int nb = (8 * num_sms + b.count - 1) / b.count;
   if (nb < 8) nb = 8;
   if (nb > kVarChunks) nb = kVarChunks;
-  if (b.elem == kElemBF16) normalize_kernel<__nv_bfloat16><<<dim3(nb, b.count), 256, 0, stream>>>(b);
-  else normalize_kernel<__half><<<dim3(nb, b.count), 256, 0, stream>>>(b);
+  // The searches that take the paired-FP16 tree get the paired copy, the others the dense one.
+  PrecisionBatch plain, paired;
+  plain.count = paired.count = 0;
+  plain.maxN = paired.maxN = b.maxN;
+  plain.elem = paired.elem = b.elem;
+  for (int k = 0; k < b.count; ++k) {
+    PrecisionBatch& dst = b.s[k].pair16 ? paired : plain;
+    dst.s[dst.count++] = b.s[k];
+  }
+  if (plain.count) {
+    if (b.elem == kElemBF16) normalize_kernel<__nv_bfloat16><<<dim3(nb, plain.count), 256, 0, stream>>>(plain);
+    else normalize_kernel<__half><<<dim3(nb, plain.count), 256, 0, stream>>>(plain);
+  }
+  if (paired.count) {
+    if (b.elem == kElemBF16) normalize_pair_kernel<__nv_bfloat16><<<dim3(nb, paired.count), 256, 0, stream>>>(paired);
+    else normalize_pair_kernel<__half><<<dim3(nb, paired.count), 256, 0, stream>>>(paired);
+  }
   return cudaGetLastError();
 }
 

@@ -50,7 +50,7 @@ def lead(R, lo, hi):
     return max(max(P) for (L, b, o), P in pos.items() if L == 1)
 
 
-def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
+def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0, h2=False):
     """Looped form: a prologue fills every node's window for step 0, then ITERS iterations
     of a U-step body; values still needed after an iteration are carried into the next
     (the loop-carried registers), and each iteration folds its U per-channel maxima into the
@@ -58,7 +58,19 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
 
     reload > 0: leaves whose window spans `reload` positions or more are not carried; each
     use reads the row again (a shared-memory load per use instead of a register per window
-    slot), which trades load bandwidth for registers and so for warps per SM."""
+    slot), which trades load bandwidth for registers and so for warps per SM.
+
+    h2: every value is a pair of FP16 sums (__half2) of two independent trees with the same
+    pairing -- two drift blocks, whose leaves the caller packs side by side -- added with
+    __hadd2 and folded with __hmax2, so one instruction does the work of two float adds; the
+    fold receives the pair."""
+    T = "__half2" if h2 else "float"
+
+    def add(x, y):
+        return f"__hadd2({x}, {y})" if h2 else f"{x} + {y}"
+
+    def mx(x, y):
+        return f"__hmax2({x}, {y})" if h2 else f"fmaxf({x}, {y})"
     pos = consumption(R, lo, hi)
     nodes = {k: (min(P), max(P)) for k, P in pos.items() if k[0] != R}  # (mn, lead)
     reloaded = {k for k, (mn, ld) in nodes.items() if reload and k[0] == 1 and ld - mn >= reload}
@@ -79,13 +91,13 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
     for (L, b, o) in order:
         mn, ld = nodes[(L, b, o)]
         if ld - mn >= 1 and (L, b, o) not in reloaded:
-            lines.append(f"  float s{nm(L, b, o)}[{ld - mn}];")
+            lines.append(f"  {T} s{nm(L, b, o)}[{ld - mn}];")
     # prologue: positions [mn, lead-1] of every node (bottom-up)
     def compute(L, b, o, j, src_pos_name):
         if L == 1:
             return f"row[{b}][{j}]"
         sh = (o + 1) // 2
-        return f"{src_pos_name(L // 2, 2 * b, o // 2, j)} + {src_pos_name(L // 2, 2 * b + 1, o // 2, j + sh)}"
+        return add(src_pos_name(L // 2, 2 * b, o // 2, j), src_pos_name(L // 2, 2 * b + 1, o // 2, j + sh))
 
     def prologue_name(L, b, o, j):
         if (L, b, o) in reloaded:
@@ -126,7 +138,7 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
                 expr = f"row[{b}][base + {j}]"
             else:
                 expr = compute(L, b, o, j, body_name)
-            body.append((j - ld, L, f"    const float {val(L, b, o, j)} = {expr};"))
+            body.append((j - ld, L, f"    const {T} {val(L, b, o, j)} = {expr};"))
     for s in range(U):
         outs = []
         for (_, _, o) in roots:
@@ -136,7 +148,7 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
             for i, e in enumerate(outs):
                 body.append((s, R, f"    sink.put({i}, base + {s}, {e});"))
             continue
-        body.append((s, R, f"    float m{s} = 0.0f;"))
+        body.append((s, R, f"    __half2 m{s} = __float2half2_rn(0.0f);" if h2 else f"    float m{s} = 0.0f;"))
         # Offsets 2q and 2q + 1 share their left operand: their larger sum is
         # left + max(right at +q, right at +q + 1), exactly (rounding is monotonic, and a NaN
         # sum never counts on either side), so the pair costs one add and one max.
@@ -147,22 +159,25 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
             if o % 2 == 0 and o + 1 in his:
                 left = body_name(R // 2, 0, q, s)
                 r0, r1 = body_name(R // 2, 1, q, s + q), body_name(R // 2, 1, q, s + q + 1)
-                outs.append(f"{left} + fmaxf({r0}, {r1})")
+                outs.append(add(left, mx(r0, r1)))
             elif o % 2 == 1 and o - 1 in his:
                 continue
             else:
                 sh = (o + 1) // 2
-                outs.append(f"{body_name(R // 2, 0, q, s)} + {body_name(R // 2, 1, q, s + sh)}")
+                outs.append(add(body_name(R // 2, 0, q, s), body_name(R // 2, 1, q, s + sh)))
         for i, e in enumerate(outs):
-            body.append((s, R, f"    const float o{s}_{i} = {e};"))
+            body.append((s, R, f"    const {T} o{s}_{i} = {e};"))
         acc = f"m{s}"
         i = 0
         while i < len(outs):
             if i + 1 < len(outs):
-                body.append((s, R + 1, f"    {acc} = fmax3({acc}, o{s}_{i}, o{s}_{i + 1});"))
+                if h2:  # no three-input form for pairs
+                    body.append((s, R + 1, f"    {acc} = __hmax2({acc}, __hmax2(o{s}_{i}, o{s}_{i + 1}));"))
+                else:
+                    body.append((s, R + 1, f"    {acc} = fmax3({acc}, o{s}_{i}, o{s}_{i + 1});"))
                 i += 2
             else:
-                body.append((s, R + 1, f"    {acc} = fmaxf({acc}, o{s}_{i});"))
+                body.append((s, R + 1, f"    {acc} = {mx(acc, f'o{s}_{i}')};"))
                 i += 1
         body.append((s, R + 2, f"    fold(mrow, base + {s}, {acc});"))
     body.sort(key=lambda x: (x[0], x[1]))
@@ -183,12 +198,13 @@ def gen_strip_loop(R, lo, hi, U, ITERS, emit=False, reload=0):
                 f"__device__ __forceinline__ void taylor_strip_emit_{R}_{lo}_{hi}_{U}_{ITERS}(\n"
                 f"    const Row (&row)[{R}], Sink& sink) {{\n{body_text}\n}}\n")
     return (f"template <typename Row, typename Fold>\n__device__ __forceinline__ void "
-            f"{loop_name(R, lo, hi, U, ITERS, reload)}(\n"
+            f"{loop_name(R, lo, hi, U, ITERS, reload, h2)}(\n"
             f"    const Row (&row)[{R}], float* __restrict__ mrow, const Fold& fold) {{\n{body_text}\n}}\n")
 
 
-def loop_name(R, lo, hi, U, ITERS, reload=0):
-    return f"taylor_strip_loop_{R}_{lo}_{hi}_{U}_{ITERS}" + (f"_r{reload}" if reload else "")
+def loop_name(R, lo, hi, U, ITERS, reload=0, h2=False):
+    return (f"taylor_strip_loop{'_h2' if h2 else ''}_{R}_{lo}_{hi}_{U}_{ITERS}" +
+            (f"_r{reload}" if reload else ""))
 
 
 def gen_direct(M, CH=1):
@@ -248,6 +264,11 @@ LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 1, 11, 3, 12),
                 (2, 1, 11, 1), (4, 1, 11, 1), (8, 1, 11, 1), (16, 2, 11, 1)]
 
 
+# (R, offset parts, U, iterations, reload) of the paired-FP16 form (two drift blocks per lane,
+# the 16-bit forms' 16-row tree).
+H2_CONFIGS = [(16, 1, 11, 3, 12), (16, 1, 11, 3, 10)]
+
+
 # (R, offset parts, U, iterations) of the emitting form: every root value goes to a sink
 # (the level kernels' output planes, through a per-warp shared-memory buffer) instead of a
 # running maximum.  Short strips (S = 11) keep a warp's buffer of one tile small.
@@ -268,6 +289,10 @@ def main(out_path):
         step = R // nparts
         for k in range(nparts):
             parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, emit=True))
+    for R, nparts, U, IT, rl in H2_CONFIGS:
+        step = R // nparts
+        for k in range(nparts):
+            parts.append(gen_strip_loop(R, k * step, (k + 1) * step, U, IT, reload=rl, h2=True))
 
     # Dispatcher: taylor_strip_loop<R, LO, HI, U, ITERS, RELOAD>(row, mrow, fold) for any element
     # accessor and fold (which merges a channel's maximum: all channels, or a range of them).
@@ -281,6 +306,16 @@ def main(out_path):
             lo, hi = k * step, (k + 1) * step
             parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT} && "
                          f"RELOAD == {rel}) {loop_name(R, lo, hi, U, IT, rel)}(row, mrow, fold);")
+    parts.append("}")
+    parts.append("template <int R, int LO, int HI, int U, int ITERS, int RELOAD, typename Row, typename Fold>\n"
+                 "__device__ __forceinline__ void taylor_strip_loop_h2(const Row (&row)[R], float* __restrict__ mrow, "
+                 "const Fold& fold) {")
+    for R, nparts, U, IT, rel in H2_CONFIGS:
+        step = R // nparts
+        for k in range(nparts):
+            lo, hi = k * step, (k + 1) * step
+            parts.append(f"  if constexpr (R == {R} && LO == {lo} && HI == {hi} && U == {U} && ITERS == {IT} && "
+                         f"RELOAD == {rel}) {loop_name(R, lo, hi, U, IT, rel, True)}(row, mrow, fold);")
     parts.append("}")
     parts.append("template <int R, int LO, int HI, int U, int ITERS, typename Row, typename Sink>\n"
                  "__device__ __forceinline__ void taylor_strip_emit(const Row (&row)[R], Sink& sink) {")

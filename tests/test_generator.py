@@ -9,7 +9,9 @@ strip): node(L, b, o)[p] = node(L/2, 2b, o/2)[p] + node(L/2, 2b+1, o/2)[p + (o+1
 
 The max-folding form must give, per channel, the maximum over its offsets floored at 0 (the
 root offsets 2q and 2q+1 are folded through their shared left operand; leaves may be read again
-instead of carried).  The emitting form must hand every root value to the sink.
+instead of carried).  The emitting form must hand every root value to the sink.  The paired-FP16
+form must give, for each of its two packed trees, the maximum of the FP16 recursion (every add
+rounded to nearest FP16, as __hadd2 does).
 """
 import os
 import re
@@ -176,3 +178,88 @@ def test_direct_level_equals_recursion(M, CH):
         assert set(got) == set(ref)
         for key, v in ref.items():
             assert np.float32(got[key]).tobytes() == v.tobytes(), (M, CH, seed, key)
+
+
+def _h16(x):
+    return np.float16(x)
+
+
+def _hadd2(a, b):
+    # the exact sum of two FP16 values fits a float64, so this rounds once, like __hadd2
+    return np.array([_h16(np.float64(a[0]) + np.float64(b[0])), _h16(np.float64(a[1]) + np.float64(b[1]))],
+                    dtype=np.float16)
+
+
+def _hmax2(a, b):
+    return np.array([max(a[0], b[0]), max(a[1], b[1])], dtype=np.float16)
+
+
+def _run_h2(code, rows2, S):
+    """Runs a generated paired-FP16 strip function: rows2[t][p] is the (2,) FP16 pair."""
+    body, depth = [], 0
+    for raw in code.splitlines():
+        st = raw.strip()
+        if (not st or st.startswith("template") or st.startswith("__device__") or st.startswith("const Row")
+                or st.startswith("#pragma")):
+            continue
+        m = re.match(r"for \(int it = 0; it < (\d+); \+\+it\) \{$", st)
+        if m:
+            body.append("    " * depth + f"for it in range({m.group(1)}):")
+            depth += 1
+            continue
+        if st == "}":
+            depth = max(0, depth - 1)
+            continue
+        st = st.rstrip(";")
+        st = re.sub(r"^__half2 (\w+)\[(\d+)\]$", r"\1 = [None] * \2", st)
+        st = re.sub(r"^__half2 (\w+) = __float2half2_rn\(0.0f\)$", r"\1 = Z2", st)
+        st = re.sub(r"^const (?:__half2|int) ", "", st)
+        st = st.replace("__hadd2(", "hadd2(").replace("__hmax2(", "hmax2(")
+        m = re.match(r"fold\(mrow, (.*), (\w+)\)$", st)
+        if m:
+            st = f"fold({m.group(1)}, {m.group(2)})"
+        body.append("    " * depth + st)
+    top = [[np.float16(0.0), np.float16(0.0)] for _ in range(S)]
+
+    def fold(i, v):
+        for h in range(2):
+            if v[h] > top[i][h]:
+                top[i][h] = v[h]
+
+    env = {"row": rows2, "Z2": np.zeros(2, dtype=np.float16), "hadd2": _hadd2, "hmax2": _hmax2, "fold": fold}
+    exec(compile("\n".join(body), "<generated>", "exec"), env)
+    return top
+
+
+def _reference_h16(rows, R, lo, hi, S):
+    memo = {}
+
+    def node(L, b, o, p):
+        key = (L, b, o, p)
+        if key not in memo:
+            if L == 1:
+                memo[key] = rows[b][p]
+            else:
+                memo[key] = _h16(np.float64(node(L // 2, 2 * b, o // 2, p)) +
+                                 np.float64(node(L // 2, 2 * b + 1, o // 2, p + (o + 1) // 2)))
+        return memo[key]
+
+    return {(o - lo, p): node(R, 0, o, p) for o in range(lo, hi) for p in range(S)}
+
+
+@pytest.mark.parametrize("R,nparts,U,IT,reload", gen.H2_CONFIGS)
+def test_paired_fp16_form_equals_fp16_recursion(R, nparts, U, IT, reload):
+    S = U * IT
+    step = R // nparts
+    for k in range(nparts):
+        lo, hi = k * step, (k + 1) * step
+        for seed in range(2):
+            a = [r.astype(np.float16) for r in _rows(R, S, 500 + 10 * k + seed)]
+            b = [r.astype(np.float16) for r in _rows(R, S, 900 + 10 * k + seed)]
+            rows2 = [np.stack([a[t], b[t]], axis=1) for t in range(R)]
+            got = _run_h2(gen.gen_strip_loop(R, lo, hi, U, IT, reload=reload, h2=True), rows2, S)
+            for h, rows in enumerate((a, b)):
+                ref = _reference_h16(rows, R, lo, hi, S)
+                for p in range(S):
+                    want = max([np.float16(0.0)] + [ref[(o - lo, p)] for o in range(lo, hi)])
+                    assert got[p][h] == want, (R, lo, hi, reload, seed, h, p, got[p][h], want)

@@ -155,3 +155,89 @@ def test_flag_bound_covers_every_channel_at_the_threshold(torch_cuda, name, x, p
     np.testing.assert_array_equal(top16[need].view(np.uint32), top32[need].view(np.uint32))
     assert h16 == h32
     assert st.recomputed_channels >= len(need)
+
+
+def _round_bf16(y32):
+    """float32 -> BF16 (round to nearest even), returned as float32 values."""
+    b = y32.view(np.uint32).astype(np.uint64)
+    b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return b.astype(np.uint32).view(np.float32)
+
+
+def _fp16_tree_top(y16, dmin, dmax):
+    """Per-channel maximum, floored at 0, of the 16-row tree in FP16 arithmetic (every add
+    rounded once to FP16, as __hadd2 does) over drift blocks dmin..dmax, leaves y16[t] read at
+    c + db*t (0 outside the band)."""
+    T, N = y16.shape
+    top = np.zeros(N, dtype=np.float16)
+    for db in range(dmin, dmax + 1):
+        rows = []
+        for t in range(T):
+            r = np.zeros(N + 64, dtype=np.float16)
+            lo, hi = max(0, -db * t), min(N, N - db * t)
+            if hi > lo:
+                r[lo:hi] = y16[t, lo + db * t:hi + db * t]
+            rows.append(r)
+        level = {(t, 0): rows[t] for t in range(T)}  # (block, offset) -> values at c
+        L = 1
+        while L < T:
+            nxt = {}
+            for b in range(T // (2 * L)):
+                for o in range(2 * L):
+                    a = level[(2 * b, o // 2)]
+                    s = (o + 1) // 2
+                    bb = np.zeros_like(a)
+                    bb[:len(a) - s] = level[(2 * b + 1, o // 2)][s:]
+                    nxt[(b, o)] = (a.astype(np.float64) + bb.astype(np.float64)).astype(np.float16)
+            level = nxt
+            L *= 2
+        for o in range(T):
+            top = np.maximum(top, level[(0, o)][:N])
+    return top.astype(np.float32)
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_paired_fp16_tree_equals_the_fp16_recursion(torch_cuda, precision):
+    """The 16-row tree of the 16-bit forms runs two drift blocks per instruction in FP16
+    pairs.  Away from the band's edges its approximate tops equal, bit for bit, the tree's
+    recursion evaluated in FP16 on the normalised copy (an odd drift-block count leaves the last
+    pair half empty); and the hits equal the FP32 form's with the pairs on and off."""
+    from seticore_b200 import Dedopplerer, _capi
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    L = _capi.lib()
+    # a drift limit of exactly k drift blocks gives 2k + 1 of them (an odd count)
+    probe = SearchSpec(16, 8192, seed=4242)
+    diag = (1e6 * probe.foff_mhz / (15 * probe.tsamp)) * 15
+    k = next(k for k in range(3, 12) if (k * diag) / abs(diag) == k)
+    spec = SearchSpec(16, 8192, max_drift=k * diag, seed=4242, n_tones=6, tone_drift=min(k * diag, 2.0),
+                      snr_threshold=8.0)
+    x = make_filterbank_numpy(spec)
+    xt = torch_cuda.from_numpy(x).cuda()
+    dd = Dedopplerer(16, 8192, spec.foff_mhz, spec.tsamp)
+    want = _hits(dd, xt, spec)
+    dd.set_precision(precision)
+    got = _hits(dd, xt, spec)
+    st = dd.last_stats()
+    top16 = dd.channel_array("top16").cpu().numpy()
+    assert got == want
+    y = (((x.astype(np.float64) - st.norm_mean) * (1.0 / st.norm_std)).astype(np.float32))
+    if precision == "bf16":
+        y = _round_bf16(y)
+    y16 = y.astype(np.float16)
+    res = 1e6 * spec.foff_mhz / (15 * spec.tsamp)
+    nmax = spec.max_drift / abs(res * 15)
+    dmin, dmax = int(np.floor(-nmax)), int(np.floor(nmax))
+    assert (dmax - dmin + 1) % 2 == 1  # an odd count: the last pair's second half is empty
+    ref = _fp16_tree_top(y16, dmin, dmax)
+    margin = 15 * max(-dmin, dmax) + 2 * 1056
+    mid = slice(margin, 8192 - margin)
+    np.testing.assert_array_equal(top16[mid], ref[mid])
+    try:
+        assert L.sc_dd_set_paired_fp16(0) == _capi.SC_DD_OK
+        assert _hits(dd, xt, spec) == want
+        flat = dd.channel_array("top16").cpu().numpy()
+        # the float-accumulating tree is within the FP16 tree's error of it
+        assert np.max(np.abs(flat[mid] - ref[mid])) <= 4 * 2.0 ** -11 * np.max(np.abs(flat[mid])) * 16
+    finally:
+        L.sc_dd_set_paired_fp16(1)
+    dd.close()
