@@ -51,6 +51,8 @@ def test_bad_arguments_are_rejected_without_gpu():
     assert lib.sc_dd_search(None, None, 0, -1, 0, 1.0, 0.0, 10.0, None, 0, ctypes.byref(n), None) == _capi.SC_DD_EINVAL
     assert lib.sc_dd_memory_usage(None) == 0
     assert lib.sc_dd_destroy(None) == _capi.SC_DD_OK
+    assert lib.sc_dd_set_paired_fp16(2) == _capi.SC_DD_EINVAL
+    assert lib.sc_dd_set_paired_fp16(1) == _capi.SC_DD_OK
 
 
 @pytest.mark.skipif(__import__("tests.conftest", fromlist=["has_gpu"]).has_gpu(), reason="checks the no-GPU path")
