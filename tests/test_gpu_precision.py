@@ -127,6 +127,11 @@ def _bound_patterns():
         out.append((f"spiky_T{T}", x))
         out.append((f"signed_T{T}", (rng.standard_normal((T, N)) * 5.0 - 1.0).astype(np.float32)))
         out.append((f"offset_T{T}", (1e4 + rng.exponential(1.0, (T, N))).astype(np.float32)))
+    # one value so far above the rest that a 16-row FP16 sum could overflow: every channel
+    # is listed and recomputed
+    x = rng.exponential(1.0, (16, 65536)).astype(np.float32)
+    x[7, 12345] = 3e7
+    out.append(("overflow_T16", x))
     return out
 
 
@@ -155,6 +160,8 @@ def test_flag_bound_covers_every_channel_at_the_threshold(torch_cuda, name, x, p
     np.testing.assert_array_equal(top16[need].view(np.uint32), top32[need].view(np.uint32))
     assert h16 == h32
     assert st.recomputed_channels >= len(need)
+    if name.startswith("overflow"):
+        assert st.recomputed_channels == st.total_channels
 
 
 def _round_bf16(y32):
