@@ -107,9 +107,10 @@ struct sc_dd {
   scb::Candidate* cands = nullptr;
   float* scratch_a = nullptr;  // Tr > 32 level buffers (one search at a time), one allocation
   float* scratch_b = nullptr;  // = scratch_a + level_buffer_floats(Tr, N)
-  // The second pair (scratch_a + 2 and 3 level_buffer_floats, same allocation) with its
-  // stream and events: every other search of a batch runs its levels there.
+  // The side streams' pairs (scratch_a + 2 + 2i and 3 + 2i level_buffer_floats, the same
+  // allocation) with their streams and events: a batch deals its level searches over them.
   scb::LevelSide side;
+  int level_pairs = 1;  // pairs of level buffers in scratch_a
   void* host = nullptr;  // pinned: slots * (header + kHostCands candidates)
   int* inc_index = nullptr;
   int* inc_steps = nullptr;
@@ -241,10 +242,12 @@ void free_all(sc_dd* d) {
   free_slots(d);
   free_prec(d);
   d->scratch_b = nullptr;  // inside scratch_a's allocation
-  dfree(d, &d->scratch_a, 4 * sizeof(float) * scb::level_buffer_floats(d->Tr, d->N));
-  if (d->side.stream) cudaStreamDestroy(d->side.stream);
+  dfree(d, &d->scratch_a, 2 * (size_t)d->level_pairs * sizeof(float) * scb::level_buffer_floats(d->Tr, d->N));
+  for (int i = 0; i < scb::kLevelSides; ++i) {
+    if (d->side.stream[i]) cudaStreamDestroy(d->side.stream[i]);
+    if (d->side.join[i]) cudaEventDestroy(d->side.join[i]);
+  }
   if (d->side.fork) cudaEventDestroy(d->side.fork);
-  if (d->side.join) cudaEventDestroy(d->side.join);
   d->side = scb::LevelSide{};
   dfree(d, &d->inc_index, sizeof(int) * d->inc_cap);
   dfree(d, &d->inc_steps, sizeof(int) * d->inc_cap);
@@ -362,7 +365,7 @@ int queue_batch(sc_dd* dd, int n, const float* const* inputs, const long long* s
       cudaGetLastError();
   };
   cudaError_t e = scb::exec_queue(es, n, dd->scratch_a, dd->scratch_b, dd->num_sms, stream, hooks,
-                                  dd->side.stream ? &dd->side : nullptr);
+                                  dd->side.n > 0 ? &dd->side : nullptr);
   if (e != cudaSuccess) return cuda_fail(e, "search kernels");
   return SC_DD_OK;
 }
@@ -604,21 +607,30 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
   // One slot; candidates for windows of 16 channels or more (grown when a call needs more).
   int rc = ensure_slots(d, 1, std::min(num_channels / 2 + 2, num_channels / 16 + 2));
   if (rc == SC_DD_OK && d->Tr > 32) {
-    // Both pairs of level buffers in one allocation: the emitting level addresses a pair as
-    // one array; the second pair serves the side stream.
+    // All pairs of level buffers in one allocation: the emitting level addresses a pair as
+    // one array; pair 0 serves the main stream, pair 1 + i side stream i.
     const size_t L = scb::level_buffer_floats(d->Tr, num_channels);
-    if ((e = dalloc(d, &d->scratch_a, 4 * sizeof(float) * L)) != cudaSuccess) {
+    const int sides = scb::level_sides();
+    d->level_pairs = 1 + sides;
+    if ((e = dalloc(d, &d->scratch_a, 2 * (size_t)d->level_pairs * sizeof(float) * L)) != cudaSuccess) {
+      d->level_pairs = 1;
       rc = fail(e == cudaErrorMemoryAllocation ? SC_DD_ENOMEM : SC_DD_ECUDA, "sc_dd_create: level buffers");
     } else {
       d->scratch_b = d->scratch_a + L;
-      d->side.lvl_a = d->scratch_a + 2 * L;
-      d->side.lvl_b = d->scratch_a + 3 * L;
-      if ((e = cudaStreamCreateWithFlags(&d->side.stream, cudaStreamNonBlocking)) != cudaSuccess ||
-          (e = cudaEventCreateWithFlags(&d->side.fork, cudaEventDisableTiming)) != cudaSuccess ||
-          (e = cudaEventCreateWithFlags(&d->side.join, cudaEventDisableTiming)) != cudaSuccess)
+      if (sides > 0 && (e = cudaEventCreateWithFlags(&d->side.fork, cudaEventDisableTiming)) != cudaSuccess)
         rc = cuda_fail(e, "sc_dd_create: level stream");
+      for (int i = 0; i < sides && rc == SC_DD_OK; ++i) {
+        d->side.lvl_a[i] = d->scratch_a + (2 + 2 * i) * L;
+        d->side.lvl_b[i] = d->scratch_a + (3 + 2 * i) * L;
+        if ((e = cudaStreamCreateWithFlags(&d->side.stream[i], cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&d->side.join[i], cudaEventDisableTiming)) != cudaSuccess)
+          rc = cuda_fail(e, "sc_dd_create: level stream");
+        else
+          d->side.n = i + 1;
+      }
     }
   }
+
   for (int i = 0; i < 4 && rc == SC_DD_OK; ++i)
     if ((e = cudaEventCreate(&d->ev[i])) != cudaSuccess) rc = cuda_fail(e, "sc_dd_create: event");
   if (rc == SC_DD_OK && ((e = cudaStreamCreateWithFlags(&d->cap_stream, cudaStreamNonBlocking)) != cudaSuccess ||

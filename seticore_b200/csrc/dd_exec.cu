@@ -9,6 +9,7 @@
 //   [flag + FP32 recompute of the flagged channels] -> hits
 #include <algorithm>
 #include <cstddef>
+#include <cstdlib>
 
 #include "dd_common.cuh"
 #include "dd_internal.h"
@@ -120,6 +121,15 @@ TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride
 
 }  // namespace
 
+int level_sides() {
+  static const int v = [] {
+    const char* e = getenv("SETICORE_B200_LEVEL_SIDES");
+    const long x = e ? strtol(e, nullptr, 10) : 1;
+    return (int)std::min<long>(kLevelSides, std::max<long>(0, x));
+  }();
+  return v;
+}
+
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
                        const ExecHooks& hooks, const LevelSide* side) {
   cudaError_t e = cudaSuccess;
@@ -209,25 +219,25 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
       }
     }
     // More than 32 rows: the level path, one search at a time per level-buffer pair.  FP32
-    // searches alternate between the main stream and the side stream, when there is one (two
-    // concurrent 16-bit level searches measured slower than one after the other: their first
-    // level is bound by L1 throughput, not by latency); the 16-bit searches run it on their
-    // normalised copy, with the default split, on the main stream.
+    // searches are dealt round-robin over the main stream and the side streams, when there are
+    // any (two concurrent 16-bit level searches measured slower than one after the other: their
+    // first level is bound by L1 throughput, not by latency); the 16-bit searches run it on
+    // their normalised copy, with the default split, on the main stream.
     int n_level = 0;
     for (int k = 0; k < m; ++k) n_level += ss[k].Tr > 32 && ss[k].elem == kElemF32;
-    const bool two = side && side->stream && n_level >= 2;
-    if (two) {
-      if ((e = cudaEventRecord(side->fork, stream)) != cudaSuccess ||
-          (e = cudaStreamWaitEvent(side->stream, side->fork, 0)) != cudaSuccess)
-        return e;
+    const int lanes = (side && side->n > 0 && n_level >= 2) ? 1 + std::min(side->n, n_level - 1) : 1;
+    if (lanes > 1) {
+      if ((e = cudaEventRecord(side->fork, stream)) != cudaSuccess) return e;
+      for (int i = 0; i + 1 < lanes; ++i)
+        if ((e = cudaStreamWaitEvent(side->stream[i], side->fork, 0)) != cudaSuccess) return e;
     }
     int j = 0;
     for (int k = 0; k < m; ++k) {
       if (ss[k].Tr <= 32) continue;
-      const bool on_side = two && ss[k].elem == kElemF32 && (j++ & 1);
-      cudaStream_t st = on_side ? side->stream : stream;
-      float* la = on_side ? side->lvl_a : lvl_a;
-      float* lb = on_side ? side->lvl_b : lvl_b;
+      const int lane = (lanes > 1 && ss[k].elem == kElemF32) ? (j++ % lanes) : 0;  // 0: the main stream
+      cudaStream_t st = lane ? side->stream[lane - 1] : stream;
+      float* la = lane ? side->lvl_a[lane - 1] : lvl_a;
+      float* lb = lane ? side->lvl_b[lane - 1] : lvl_b;
       if (ss[k].elem != kElemF32) {
         if ((e = levels_search(ss[k].norm16, ss[k].N, ss[k].Tr, ss[k].N, ss[k].dmin, ss[k].dmax, la, lb, ss[k].top16,
                                num_sms, st, LevelPlan{}, ss[k].elem, header_status(ss[k]))) != cudaSuccess)
@@ -239,9 +249,9 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
                              ss[k].top, num_sms, st, plan, kElemF32, header_status(ss[k]))) != cudaSuccess)
         return e;
     }
-    if (two) {
-      if ((e = cudaEventRecord(side->join, side->stream)) != cudaSuccess ||
-          (e = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess)
+    for (int i = 0; i + 1 < lanes; ++i) {
+      if ((e = cudaEventRecord(side->join[i], side->stream[i])) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(stream, side->join[i], 0)) != cudaSuccess)
         return e;
     }
     if (hooks.after_tree) hooks.after_tree(hooks.ctx, stream);

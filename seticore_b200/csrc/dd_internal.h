@@ -398,22 +398,27 @@ struct ExecHooks {
   void (*after_tree)(void* ctx, cudaStream_t s) = nullptr;
 };
 
-// A second stream with its own level buffers (the same size as the first pair, in one
-// allocation) and two events: exec_queue then runs every other search of more than 32 rows
-// on it, forked from and joined back into the main stream, so that the level kernels of two
+// Up to kLevelSides more streams, each with its own pair of level buffers (the same size as
+// the first pair, in one allocation), a fork event and join events: exec_queue then deals the
+// FP32 searches of more than 32 rows round-robin over the main stream and the side streams,
+// forked from and joined back into the main stream, so that the level kernels of several
 // searches share the SMs (they are bound by latency, with shared memory and registers the
 // respective limits).
+constexpr int kLevelSides = 3;
 struct LevelSide {
-  cudaStream_t stream = nullptr;
-  float* lvl_a = nullptr;
-  float* lvl_b = nullptr;
+  int n = 0;  // side streams in use
+  cudaStream_t stream[kLevelSides] = {};
+  float* lvl_a[kLevelSides] = {};
+  float* lvl_b[kLevelSides] = {};
   cudaEvent_t fork = nullptr;
-  cudaEvent_t join = nullptr;
+  cudaEvent_t join[kLevelSides] = {};
 };
+// Side streams an engine or pool creates (SETICORE_B200_LEVEL_SIDES, 0 to 3; default 1).
+int level_sides();
 
 // Queues every kernel of n searches (any mix) on `stream`; no synchronisation.
 // lvl_a / lvl_b: level buffers of level_buffer_floats(Tr, N) floats for every search with
-// Tr > 32, in one allocation.  side: optional second stream for the level path.
+// Tr > 32, in one allocation.  side: optional side streams for the level path.
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,
                        const ExecHooks& hooks, const LevelSide* side = nullptr);
 

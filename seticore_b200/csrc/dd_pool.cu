@@ -74,7 +74,7 @@ struct sc_dd_pool {
   float* lvl_a = nullptr;
   float* lvl_b = nullptr;
   size_t lvl_floats = 0;
-  scb::LevelSide side;  // its buffers: lvl_a + 2 and 3 lvl_floats, the same allocation
+  scb::LevelSide side;  // side stream i's buffers: lvl_a + 2 + 2i and 3 + 2i lvl_floats
   char* host = nullptr;  // pinned: headers + candidate heads of the largest sub-batch
   size_t host_bytes = 0;
   cudaStream_t cap_stream = nullptr;
@@ -252,15 +252,20 @@ int ensure_device(sc_dd_pool* p, size_t arena, size_t lvl, cudaStream_t stream) 
   }
   if (lvl > p->lvl_floats) {
     if (p->lvl_a) cudaFreeAsync(p->lvl_a, stream);
-    p->lvl_a = p->lvl_b = p->side.lvl_a = p->side.lvl_b = nullptr;
+    p->lvl_a = p->lvl_b = nullptr;
+    for (int i = 0; i < scb::kLevelSides; ++i) p->side.lvl_a[i] = p->side.lvl_b[i] = nullptr;
     p->lvl_floats = 0;
-    // Both pairs of level buffers in one allocation: the emitting level addresses a pair as
-    // one array; the second pair serves the side stream.
-    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&p->lvl_a), 4 * lvl * sizeof(float), stream)) != cudaSuccess)
+    // All pairs of level buffers in one allocation: the emitting level addresses a pair as
+    // one array; pair 0 serves the pool's stream, pair 1 + i side stream i.
+    const size_t pairs = 1 + (size_t)p->side.n;
+    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&p->lvl_a), 2 * pairs * lvl * sizeof(float), stream)) !=
+        cudaSuccess)
       return pfail(SC_DD_ENOMEM, std::string("pool level buffers: ") + cudaGetErrorString(e));
     p->lvl_b = p->lvl_a + lvl;
-    p->side.lvl_a = p->lvl_a + 2 * lvl;
-    p->side.lvl_b = p->lvl_a + 3 * lvl;
+    for (int i = 0; i < p->side.n; ++i) {
+      p->side.lvl_a[i] = p->lvl_a + (2 + 2 * i) * lvl;
+      p->side.lvl_b[i] = p->lvl_a + (3 + 2 * i) * lvl;
+    }
     p->lvl_floats = lvl;
   }
   return SC_DD_OK;
@@ -276,7 +281,7 @@ cudaError_t queue_sub(sc_dd_pool* p, std::vector<Planned>& sub, cudaStream_t s) 
   hooks.level_plan = pool_level_plan;
   // The tuner times one level search at a time on its own stream: no side stream then.
   cudaError_t e = scb::exec_queue(es.data(), (int)es.size(), p->lvl_a, p->lvl_b, p->num_sms, s, hooks,
-                                  p->tuning_now ? nullptr : &p->side);
+                                  p->tuning_now || p->side.n == 0 ? nullptr : &p->side);
   if (e != cudaSuccess) return e;
   char* h = p->host;
   for (size_t k = 0; k < sub.size(); ++k) {
@@ -306,9 +311,12 @@ int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out) {
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side.stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->side.join, cudaEventDisableTiming);
+  if (e == cudaSuccess && scb::level_sides() > 0) e = cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming);
+  for (int i = 0; i < scb::level_sides() && e == cudaSuccess; ++i) {
+    if ((e = cudaStreamCreateWithFlags(&p->side.stream[i], cudaStreamNonBlocking)) == cudaSuccess &&
+        (e = cudaEventCreateWithFlags(&p->side.join[i], cudaEventDisableTiming)) == cudaSuccess)
+      p->side.n = i + 1;
+  }
   for (cudaEvent_t* ev : {&p->ev0, &p->ev1, &p->evj, &p->t0, &p->t1})
     if (e == cudaSuccess) e = cudaEventCreate(ev);
   // The host buffer of the largest possible sub-batch, allocated once: pinned allocations
@@ -317,10 +325,13 @@ int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out) {
   if (e == cudaSuccess) e = cudaMallocHost(&p->host, p->host_bytes);
   if (e != cudaSuccess) {
     if (p->host) cudaFreeHost(p->host);
-    for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1, p->side.fork, p->side.join})
+    for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1, p->side.fork})
       if (ev) cudaEventDestroy(ev);
-    for (cudaStream_t st : {p->cap_stream, p->side.stream})
-      if (st) cudaStreamDestroy(st);
+    if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+    for (int i = 0; i < scb::kLevelSides; ++i) {
+      if (p->side.stream[i]) cudaStreamDestroy(p->side.stream[i]);
+      if (p->side.join[i]) cudaEventDestroy(p->side.join[i]);
+    }
     delete p;
     return pcuda(e, "sc_dd_pool_create");
   }
@@ -341,9 +352,11 @@ int sc_dd_pool_destroy(sc_dd_pool* p) {
   for (cudaEvent_t ev : {p->ev0, p->ev1, p->evj, p->t0, p->t1})
     if (ev) cudaEventDestroy(ev);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
-  if (p->side.stream) cudaStreamDestroy(p->side.stream);
-  for (cudaEvent_t ev : {p->side.fork, p->side.join})
-    if (ev) cudaEventDestroy(ev);
+  for (int i = 0; i < scb::kLevelSides; ++i) {
+    if (p->side.stream[i]) cudaStreamDestroy(p->side.stream[i]);
+    if (p->side.join[i]) cudaEventDestroy(p->side.join[i]);
+  }
+  if (p->side.fork) cudaEventDestroy(p->side.fork);
   delete p;
   return SC_DD_OK;
 }
