@@ -192,7 +192,7 @@ int sc_dd_set_level_stripe_bytes(long long bytes);
 int sc_dd_set_exact_statistics(int mode);
 
 /* No counterpart in the reference (which has no 16-bit form).  on 1 (the default): the BF16
- * and FP16 forms' searches of 16 rounded timesteps run their approximate tree in FP16 pairs,
+ * and FP16 forms' searches of 16 or 32 rounded timesteps run their approximate tree in FP16 pairs,
  * two drift blocks per instruction; the flag bound then covers FP16 adds, so a few more
  * channels are recomputed in float32.  on 0: that tree accumulates in float32.  The hit
  * lists are identical either way.  Process-wide; launches queued after the call follow it (a

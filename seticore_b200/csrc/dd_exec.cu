@@ -63,8 +63,9 @@ SearchDesc to_desc(const ExecSearch& e) {
   return s;
 }
 
-// 16-bit 16-row searches take the paired-FP16 tree when it is on (the flag bound must know).
-bool pair16_search(const ExecSearch& e, bool on) { return on && e.elem != kElemF32 && e.Tr == 16; }
+// 16-bit 16- and 32-row searches take the paired-FP16 tree when it is on (the flag bound must
+// know).
+bool pair16_search(const ExecSearch& e, bool on) { return on && e.elem != kElemF32 && pair_rows(e.Tr); }
 
 PrecisionDesc to_pdesc(const ExecSearch& e, const SearchHeader* hdr, bool pair_on) {
   PrecisionDesc q{};
@@ -193,7 +194,7 @@ cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, i
         TreeBatch tb;
         tb.count = 0;
         tb.n_items = 0;
-        tb.pair16 = (elem != kElemF32 && R == 16 && pair_on) ? 1 : 0;
+        tb.pair16 = (elem != kElemF32 && pair_rows(R) && pair_on) ? 1 : 0;
         for (int k = 0; k < m; ++k) {
           if (ss[k].Tr != R || ss[k].elem != elem) continue;
           if (elem == kElemF32) {

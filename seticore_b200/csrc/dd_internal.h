@@ -174,14 +174,15 @@ struct TreeBatch {
   // L2 hints of the bulk copies: 0 none; 1 (stripe passes' first level) staged input rows
   // evict-first and emitted planes evict-last, so the planes stay in L2 for the last level.
   int cache_mode = 0;
-  // 1: the groups are 16-bit rows of 16-row searches, run by the paired-FP16 tree (two drift
-  // blocks per unit, FP16 sums; the precision form's flag bound then takes FP16 adds).
+  // 1: the groups are the paired copies of 16-bit 16- or 32-row searches, run by the
+  // paired-FP16 tree (two drift blocks per unit, FP16 sums; the precision form's flag bound
+  // then takes FP16 adds).
   int pair16 = 0;
   TreeGroup g[kMaxBatch];
 };
 
-// Whether 16-bit 16-row searches queued from now on take the paired-FP16 tree (default on;
-// off: the float-accumulating 16-bit tree).  The hit lists are the same either way.
+// Whether 16-bit 16- and 32-row searches queued from now on take the paired-FP16 tree (default
+// on; off: the float-accumulating 16-bit tree).  The hit lists are the same either way.
 void set_paired_fp16(bool on);
 bool paired_fp16();
 
@@ -227,16 +228,18 @@ inline long long level_row_length(int N) {
 // four drift blocks of a last level of up to 16 rows, dd_levels.cu), so the two level
 // buffers hold a whole-row pass of two drift blocks.
 constexpr long long kLevelRowSlack = 2048;
-// The paired-FP16 copy of a 16-row search (the 16-bit forms' paired tree): row t holds, for
-// channel x in [-kPairPad, N), the word (y[t][x], y[t][x + t]) as two FP16 values (0 outside
-// [0, N)), kPairPad words before channel 0 and rows pair_row_words(N) words apart.
-constexpr int kPairPad = 16;
+// The paired-FP16 copy of a 16- or 32-row search (the 16-bit forms' paired tree): row t
+// holds, for channel x in [-kPairPad, N), the word (y[t][x], y[t][x + t]) as two FP16 values
+// (0 outside [0, N)), kPairPad words before channel 0 (at least the largest shift, 31) and
+// rows pair_row_words(N) words apart.
+constexpr int kPairPad = 32;
 inline long long pair_row_words(int N) { return ((long long)N + kPairPad + 3) / 4 * 4; }
-// Bytes of a search's normalised copy: the dense 16-bit [Tr][N] copy, or for 16 rows room
-// for the paired copy as well (whichever the paired-FP16 setting picks at launch).
+inline bool pair_rows(int Tr) { return Tr == 16 || Tr == 32; }
+// Bytes of a search's normalised copy: the dense 16-bit [Tr][N] copy, or for 16 and 32 rows
+// room for the paired copy as well (whichever the paired-FP16 setting picks at launch).
 inline size_t norm_buffer_bytes(int Tr, int N) {
   const size_t dense = (size_t)2 * Tr * N;
-  const size_t paired = Tr == 16 ? (size_t)4 * Tr * (size_t)pair_row_words(N) : 0;
+  const size_t paired = pair_rows(Tr) ? (size_t)4 * Tr * (size_t)pair_row_words(N) : 0;
   return dense > paired ? dense : paired;
 }
 

@@ -246,19 +246,21 @@ __device__ __forceinline__ unsigned short pair_bits(float y) {
   }
 }
 
-// The paired copy of a 16-row search (the paired-FP16 tree's input): the same single read as
-// normalize_kernel -- y in FP64, rounded to the storage form, the float32 column sums in row
-// order and the extremes -- but it writes, for row t and channel x in [-kPairPad, N), the word
-// (y[t][x], y[t][x + t]) as two FP16 values (0 outside [0, N)): the leaves of drift blocks k
-// and k + 1 side by side, since the tree reads row t of drift block k + 1 t channels further.
-// A block takes kPairCols channels at a time, four per thread (256 threads): their values,
-// and those of the next kPairPad channels, go to shared memory, then every word of its
-// channels is written whole (16-byte stores).
+// The paired copy of a 16- or 32-row search (the paired-FP16 tree's input): the same single
+// read as normalize_kernel -- y in FP64, rounded to the storage form, the float32 column sums
+// in row order and the extremes -- but it writes, for row t and channel x in [-kPairPad, N),
+// the word (y[t][x], y[t][x + t]) as two FP16 values (0 outside [0, N)): the leaves of drift
+// blocks k and k + 1 side by side, since the tree reads row t of drift block k + 1 t channels
+// further.  A block takes kPairCols channels at a time, four per thread (256 threads), and
+// the rows sixteen at a time: their values, and those of the next kPairPad channels, go to
+// shared memory, then every word of those rows is written whole (16-byte stores).
 constexpr int kPairCols = 1024;
-template <typename E>
+template <typename E, int TR>
 __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_constant__ PrecisionBatch b) {
+  static_assert(TR == 16 || TR == 32, "paired copies hold 16 or 32 rows");
   const PrecisionDesc& d = b.s[blockIdx.y];
-  // rows of kPairCols + kPairPad values; 2080 bytes, so every 4-value group is 8-byte aligned
+  // sixteen rows of kPairCols + kPairPad values (2112 bytes: every 4-value group is 8-byte
+  // aligned)
   __shared__ __align__(16) unsigned short ys[16][kPairCols + kPairPad];
   const double mean = d.moments[2 * kVarChunks];
   const double inv = 1.0 / d.moments[2 * kVarChunks + 1];
@@ -268,56 +270,92 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
   float mn = __int_as_float(0x7f800000), mx = -mn;  // NaNs are skipped (they flag themselves)
   const bool vec = (N % 4 == 0) && (d.row_stride % 4 == 0) && ((reinterpret_cast<uintptr_t>(d.input) & 15) == 0);
   for (long long c0 = (long long)blockIdx.x * kPairCols; c0 < N; c0 += (long long)gridDim.x * kPairCols) {
-    // the next kPairPad channels' values (the second elements of the last words): one value
-    // per thread, issued before the block's own loads
-    {
-      const int t = threadIdx.x >> 4, i = threadIdx.x & 15;
-      const long long x = c0 + kPairCols + i;
-      unsigned short h = 0;
-      if (x < N && t < T) h = pair_bits<E>((float)(((double)__ldg(d.input + (long long)t * d.row_stride + x) - mean) * inv));
-      ys[t][kPairCols + i] = h;
-    }
-    // four channels per thread down the 16 rows, eight rows' loads in flight at a time;
-    // channels past N are 0 and do not enter the sums or the extremes
     const long long c = c0 + 4 * threadIdx.x;
     const bool full = vec && c + 3 < N;
     const int nin = c >= N ? 0 : (c + 3 < N ? 4 : (int)(N - c));
     float cs[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+    for (int g = 0; g < TR; g += 16) {
+      // the next kPairPad channels' values of these rows (the second elements of the last
+      // words): two per thread, issued before the block's own loads
 #pragma unroll
-    for (int g = 0; g < 16; g += 8) {
-      float e[8][4];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const float* row = d.input + (long long)(g + u) * d.row_stride;
-        if (full) {
-          const float4 q = __ldg(reinterpret_cast<const float4*>(row + c));
-          e[u][0] = q.x;
-          e[u][1] = q.y;
-          e[u][2] = q.z;
-          e[u][3] = q.w;
-        } else {
-#pragma unroll
-          for (int i = 0; i < 4; ++i) e[u][i] = i < nin ? __ldg(row + c + i) : 0.0f;
-        }
+      for (int h = 0; h < 2; ++h) {
+        const int v = threadIdx.x + 256 * h;
+        const int u = v >> 5, i = v & 31;
+        const long long x = c0 + kPairCols + i;
+        unsigned short hv = 0;
+        if (x < N && g + u < T)
+          hv = pair_bits<E>((float)(((double)__ldg(d.input + (long long)(g + u) * d.row_stride + x) - mean) * inv));
+        ys[u][kPairCols + i] = hv;
       }
+      // four channels per thread down the sixteen rows, eight rows' loads in flight at a
+      // time; channels past N are 0 and do not enter the sums or the extremes
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int t = g + u;
-        unsigned long long packed = 0;
+      for (int g8 = 0; g8 < 16; g8 += 8) {
+        float e[8][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) cs[i] += e[u][i];
-        if (t < T) {
+        for (int u = 0; u < 8; ++u) {
+          const float* row = d.input + (long long)(g + g8 + u) * d.row_stride;
+          if (full) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(row + c));
+            e[u][0] = q.x;
+            e[u][1] = q.y;
+            e[u][2] = q.z;
+            e[u][3] = q.w;
+          } else {
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            if (i < nin) {
-              packed |= (unsigned long long)pair_bits<E>((float)(((double)e[u][i] - mean) * inv)) << (16 * i);
-              mn = fminf(mn, e[u][i]);
-              mx = fmaxf(mx, e[u][i]);
-            }
+            for (int i = 0; i < 4; ++i) e[u][i] = i < nin ? __ldg(row + c + i) : 0.0f;
           }
         }
-        *reinterpret_cast<unsigned long long*>(&ys[t][4 * threadIdx.x]) = packed;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int t = g + g8 + u;
+          unsigned long long packed = 0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) cs[i] += e[u][i];
+          if (t < T) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              if (i < nin) {
+                packed |= (unsigned long long)pair_bits<E>((float)(((double)e[u][i] - mean) * inv)) << (16 * i);
+                mn = fminf(mn, e[u][i]);
+                mx = fmaxf(mx, e[u][i]);
+              }
+            }
+          }
+          *reinterpret_cast<unsigned long long*>(&ys[g8 + u][4 * threadIdx.x]) = packed;
+        }
       }
+      __syncthreads();
+      // words (y[t][j], y[t][j + t]): the second values are the four starting t further, taken
+      // from two aligned 8-byte loads by a constant shift (the loop is unrolled over u; t's
+      // low two bits are u's)
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int t = g + u;
+        const int sh = t & ~3;  // g is a multiple of 16, so t & 3 == u & 3
+        const unsigned long long lo = *reinterpret_cast<const unsigned long long*>(&ys[u][4 * threadIdx.x]);
+        const unsigned long long ha = *reinterpret_cast<const unsigned long long*>(&ys[u][4 * threadIdx.x + sh]);
+        const unsigned long long hb = *reinterpret_cast<const unsigned long long*>(&ys[u][4 * threadIdx.x + sh + 4]);
+        const unsigned long long hi = (u & 3) ? (ha >> (16 * (u & 3))) | (hb << (64 - 16 * (u & 3))) : ha;
+        const uint32_t l0 = (uint32_t)lo, l1 = (uint32_t)(lo >> 32), h0 = (uint32_t)hi, h1 = (uint32_t)(hi >> 32);
+        const uint4 w = make_uint4(__byte_perm(l0, h0, 0x5410), __byte_perm(l0, h0, 0x7632),
+                                   __byte_perm(l1, h1, 0x5410), __byte_perm(l1, h1, 0x7632));
+        uint32_t* dst = out + (long long)t * np + kPairPad + c;
+        if (nin == 4) {
+          *reinterpret_cast<uint4*>(dst) = w;
+        } else {
+          const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+          for (int i = 0; i < nin; ++i) dst[i] = ws[i];
+        }
+      }
+      // the kPairPad words before channel 0: (0, y[t][x + t])
+      if (c0 == 0 && threadIdx.x < 16) {
+        const int u = threadIdx.x, t = g + u;
+        for (int x = -kPairPad; x < 0; ++x)
+          out[(long long)t * np + kPairPad + x] = x + t >= 0 ? (uint32_t)ys[u][x + t] << 16 : 0u;
+      }
+      __syncthreads();
     }
     if (d.colsum) {
       if (nin == 4) {
@@ -326,33 +364,6 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
         for (int i = 0; i < nin; ++i) d.colsum[c + i] = cs[i];
       }
     }
-    __syncthreads();
-    // words (y[t][j], y[t][j + t]): the second values are the four starting t further, taken
-    // from two aligned 8-byte loads by a constant shift (t is unrolled)
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const unsigned long long lo = *reinterpret_cast<const unsigned long long*>(&ys[t][4 * threadIdx.x]);
-      const unsigned long long ha = *reinterpret_cast<const unsigned long long*>(&ys[t][4 * threadIdx.x + (t & ~3)]);
-      const unsigned long long hb = *reinterpret_cast<const unsigned long long*>(&ys[t][4 * threadIdx.x + (t & ~3) + 4]);
-      const unsigned long long hi = (t & 3) ? (ha >> (16 * (t & 3))) | (hb << (64 - 16 * (t & 3))) : ha;
-      const uint32_t l0 = (uint32_t)lo, l1 = (uint32_t)(lo >> 32), h0 = (uint32_t)hi, h1 = (uint32_t)(hi >> 32);
-      const uint4 w = make_uint4(__byte_perm(l0, h0, 0x5410), __byte_perm(l0, h0, 0x7632), __byte_perm(l1, h1, 0x5410),
-                                 __byte_perm(l1, h1, 0x7632));
-      uint32_t* dst = out + (long long)t * np + kPairPad + c;
-      if (nin == 4) {
-        *reinterpret_cast<uint4*>(dst) = w;
-      } else {
-        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-        for (int i = 0; i < nin; ++i) dst[i] = ws[i];
-      }
-    }
-    // the kPairPad words before channel 0: (0, y[t][x + t])
-    if (c0 == 0 && threadIdx.x < 16) {
-      const int t = threadIdx.x;
-      for (int x = -kPairPad; x < 0; ++x)
-        out[(long long)t * np + kPairPad + x] = x + t >= 0 ? (uint32_t)ys[t][x + t] << 16 : 0u;
-    }
-    __syncthreads();
   }
   double a, q, omn, omx;
   if (!fold_moments(d, 0.0, 0.0, mn, mx, &a, &q, &omn, &omx)) return;
@@ -520,9 +531,23 @@ cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
     if (b.elem == kElemBF16) normalize_kernel<__nv_bfloat16><<<dim3(nb, plain.count), 256, 0, stream>>>(plain);
     else normalize_kernel<__half><<<dim3(nb, plain.count), 256, 0, stream>>>(plain);
   }
-  if (paired.count) {
-    if (b.elem == kElemBF16) normalize_pair_kernel<__nv_bfloat16><<<dim3(nb, paired.count), 256, 0, stream>>>(paired);
-    else normalize_pair_kernel<__half><<<dim3(nb, paired.count), 256, 0, stream>>>(paired);
+  // paired copies, one launch per row count
+  for (int tr : {16, 32}) {
+    PrecisionBatch q;
+    q.count = 0;
+    q.maxN = b.maxN;
+    q.elem = b.elem;
+    for (int k = 0; k < paired.count; ++k)
+      if (paired.s[k].Tr == tr) q.s[q.count++] = paired.s[k];
+    if (!q.count) continue;
+    const dim3 grid(nb, q.count);
+    if (b.elem == kElemBF16) {
+      if (tr == 16) normalize_pair_kernel<__nv_bfloat16, 16><<<grid, 256, 0, stream>>>(q);
+      else normalize_pair_kernel<__nv_bfloat16, 32><<<grid, 256, 0, stream>>>(q);
+    } else {
+      if (tr == 16) normalize_pair_kernel<__half, 16><<<grid, 256, 0, stream>>>(q);
+      else normalize_pair_kernel<__half, 32><<<grid, 256, 0, stream>>>(q);
+    }
   }
   return cudaGetLastError();
 }

@@ -265,8 +265,8 @@ LOOP_CONFIGS = [(2, 1, 11, 3), (4, 1, 11, 3), (8, 1, 11, 3), (16, 1, 11, 3, 12),
 
 
 # (R, offset parts, U, iterations, reload) of the paired-FP16 form (two drift blocks per lane,
-# the 16-bit forms' 16-row tree).
-H2_CONFIGS = [(16, 1, 11, 3, 12), (16, 1, 11, 3, 10)]
+# the 16-bit forms' 16- and 32-row trees).
+H2_CONFIGS = [(16, 1, 11, 3, 12), (16, 1, 11, 3, 10), (32, 2, 11, 3, 0)]
 
 
 # (R, offset parts, U, iterations) of the emitting form: every root value goes to a sink

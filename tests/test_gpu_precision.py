@@ -203,24 +203,26 @@ def _fp16_tree_top(y16, dmin, dmax):
     return top.astype(np.float32)
 
 
+@pytest.mark.parametrize("T", [16, 32])
 @pytest.mark.parametrize("precision", ["fp16", "bf16"])
-def test_paired_fp16_tree_equals_the_fp16_recursion(torch_cuda, precision):
-    """The 16-row tree of the 16-bit forms runs two drift blocks per instruction in FP16
-    pairs.  Away from the band's edges its approximate tops equal, bit for bit, the tree's
+def test_paired_fp16_tree_equals_the_fp16_recursion(torch_cuda, precision, T):
+    """The 16- and 32-row trees of the 16-bit forms run two drift blocks per instruction in
+    FP16 pairs.  Away from the band's edges its approximate tops equal, bit for bit, the tree's
     recursion evaluated in FP16 on the normalised copy (an odd drift-block count leaves the last
     pair half empty); and the hits equal the FP32 form's with the pairs on and off."""
     from seticore_b200 import Dedopplerer, _capi
     from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
     L = _capi.lib()
     # a drift limit of exactly k drift blocks gives 2k + 1 of them (an odd count)
-    probe = SearchSpec(16, 8192, seed=4242)
-    diag = (1e6 * probe.foff_mhz / (15 * probe.tsamp)) * 15
+    tsamp = 18.253611 * 16 / T
+    probe = SearchSpec(T, 8192, seed=4242, tsamp=tsamp)
+    diag = (1e6 * probe.foff_mhz / ((T - 1) * probe.tsamp)) * (T - 1)
     k = next(k for k in range(3, 12) if (k * diag) / abs(diag) == k)
-    spec = SearchSpec(16, 8192, max_drift=k * diag, seed=4242, n_tones=6, tone_drift=min(k * diag, 2.0),
-                      snr_threshold=8.0)
+    spec = SearchSpec(T, 8192, max_drift=k * diag, seed=4242, n_tones=6, tone_drift=min(k * diag, 2.0),
+                      snr_threshold=8.0, tsamp=tsamp)
     x = make_filterbank_numpy(spec)
     xt = torch_cuda.from_numpy(x).cuda()
-    dd = Dedopplerer(16, 8192, spec.foff_mhz, spec.tsamp)
+    dd = Dedopplerer(T, 8192, spec.foff_mhz, spec.tsamp)
     want = _hits(dd, xt, spec)
     dd.set_precision(precision)
     got = _hits(dd, xt, spec)
@@ -231,12 +233,12 @@ def test_paired_fp16_tree_equals_the_fp16_recursion(torch_cuda, precision):
     if precision == "bf16":
         y = _round_bf16(y)
     y16 = y.astype(np.float16)
-    res = 1e6 * spec.foff_mhz / (15 * spec.tsamp)
-    nmax = spec.max_drift / abs(res * 15)
+    res = 1e6 * spec.foff_mhz / ((T - 1) * spec.tsamp)
+    nmax = spec.max_drift / abs(res * (T - 1))
     dmin, dmax = int(np.floor(-nmax)), int(np.floor(nmax))
     assert (dmax - dmin + 1) % 2 == 1  # an odd count: the last pair's second half is empty
     ref = _fp16_tree_top(y16, dmin, dmax)
-    margin = 15 * max(-dmin, dmax) + 2 * 1056
+    margin = (T - 1) * max(-dmin, dmax) + 2 * 1056
     mid = slice(margin, 8192 - margin)
     np.testing.assert_array_equal(top16[mid], ref[mid])
     try:
@@ -244,7 +246,7 @@ def test_paired_fp16_tree_equals_the_fp16_recursion(torch_cuda, precision):
         assert _hits(dd, xt, spec) == want
         flat = dd.channel_array("top16").cpu().numpy()
         # the float-accumulating tree is within the FP16 tree's error of it
-        assert np.max(np.abs(flat[mid] - ref[mid])) <= 4 * 2.0 ** -11 * np.max(np.abs(flat[mid])) * 16
+        assert np.max(np.abs(flat[mid] - ref[mid])) <= 5 * 2.0 ** -11 * np.max(np.abs(flat[mid])) * T
     finally:
         L.sc_dd_set_paired_fp16(1)
     dd.close()
