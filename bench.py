@@ -44,18 +44,18 @@ METRIC = "dedoppler Gsamples/s (FP32, 64 coarse x 16 x 2^20 node)"
 UNIT = "Gsamples/s"
 # DRAM bytes per searched coarse channel in the tree kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture of a launch over 4 coarse channels: 285.93 MB +
-# 27.68 MB; profiles/tree_max_kernel_node.md); a launch covering k coarse channels moves k
-# times this.
+# 27.68 MB, with the command that made it in the tree kernel's profile summary); a launch
+# covering k coarse channels moves k times this.
 TREE_DRAM_BYTES = 78400384
 # Warp instructions the tree kernel executes per coarse channel of the node (ncu
 # smsp__inst_executed.sum of the same capture: 748.2 M for 4 coarse channels).
 TREE_WARP_INSTR = 748.2e6 / 4
 # Level path of the beams workload, DRAM bytes per beam of 256 x 131072 (2 drift blocks, one
 # whole-row pass): the emitting first level 134.3 + 213.1 MB and the last level 269.5 + 3.9 MB
-# (ncu, one launch each; profiles/level_kernels_beams.md).
+# (ncu, one launch each, summarised with the level kernels' profile).
 BEAMS_DRAM_BYTES = 620.7e6
 # Kernels of one FP32 batch of up to 64 searches of 2^20 channels and at most 32 rows (the
-# launch list of one node step, profiles/launch_list_node.md): clear, tree, range, three
+# launch list of one node step under ncu): clear, tree, range, three
 # histogram passes, compaction, order-statistic finish, two variance kernels, window, drift
 # recovery, and the exact statistics' launches, which exit at once when no search needs them
 # (reset, init, 15 partition rounds of three launches, two finishers, moments).
@@ -641,12 +641,12 @@ def main():
                 "algorithmic_bytes_note": "input read once + top sums and column sums written, 4*Tr*N + 8*N "
                                           "per search",
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per coarse channel "
-                                  "(profiles/tree_max_kernel_node.md) x searches per launch",
+                                  "(one capture of a 4-channel launch) x searches per launch",
                 "traffic_frac": traffic / (tree_launch_ms / 1e3) / 1e9 / peak,
                 "binding_limit": "instruction issue",
                 "issue_roof": {"warp_instructions_per_launch": TREE_WARP_INSTR * per_launch, "sms": sms,
                                "sm_mhz": sm_mhz, "roof_ms": issue_roof_ms, "frac": issue_roof_ms / tree_launch_ms,
-                               "source": "ncu smsp__inst_executed.sum (profiles/tree_max_kernel_node.md)"},
+                               "source": "ncu smsp__inst_executed.sum (one capture of a 4-channel launch)"},
                 "bytes_if_read_per_drift_block": bytes_read_per_drift_block(T, N, ndb) * per_launch,
                 "bytes_if_read_per_drift_block_note": "the reference's schedule (one input read per drift "
                                                       "block); not a bound for the fused kernel"}
