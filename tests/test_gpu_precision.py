@@ -118,7 +118,7 @@ def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle, name):
 def _bound_patterns():
     rng = np.random.default_rng(77)
     out = []
-    for T, N in ((16, 65536), (64, 20000)):
+    for T, N in ((16, 65536), (32, 32768), (64, 20000)):
         out.append((f"exponential_T{T}", rng.exponential(1.0, (T, N)).astype(np.float32)))
         out.append((f"heavy_tail_T{T}", (rng.exponential(1.0, (T, N)) ** 4).astype(np.float32)))
         x = rng.exponential(1.0, (T, N)).astype(np.float32)
