@@ -295,9 +295,10 @@ def run_uneven(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
-# Serving shape: three workers (streams) and batches of at most 1e8 samples.  On the uneven mix
-# this measured capacity 55.7 Gsamples/s with p50 / p99 of 6.9 / 15.6 ms at 1.0x load, against
-# 62.0 with 11.0 / 28.6 ms for two workers and batches bounded only by 64 requests.
+# Serving shape: three workers (streams) and batches of at most 1e8 samples while the queue is
+# short (the cap grows to a third of the queued samples when more waits).  On the uneven mix
+# this measured capacity 57.5 Gsamples/s with p50 / p99 of 9.1 / 24.9 ms at 1.0x load; a fixed
+# cap 48.0-55.7 with 6.9-7.4 / 15.6-16.7 ms; no cap and two workers 62.0 with 11.0 / 28.6 ms.
 SERVE_WORKERS = 3
 SERVE_BATCH_SAMPLES = 100_000_000
 
@@ -318,7 +319,8 @@ def serve_result(world, rank, local, n_inputs, serve_seconds):
     out = {"metric": "serving p50/p99 latency and Gsamples/s (uneven mix)", "unit": "s", "n_gpus": world,
            "data": "synthetic", "higher_is_better": False,
            "config": {"workload": f"serve: {n_inputs} resident inputs from the uneven mix, Poisson arrivals, "
-                                  "120 GB HBM budget, 3 workers, at most 64 requests and 1e8 samples per batch",
+                                  "120 GB HBM budget, 3 workers, at most 64 requests and 1e8 samples per batch "
+                                  "(or a third of the queued samples, if more)",
                       "budget_bytes": budget, "workers": SERVE_WORKERS, "max_batch_samples": SERVE_BATCH_SAMPLES},
            "forms": {}}
     for form in ["fp32", "bf16"]:

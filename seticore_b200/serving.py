@@ -43,6 +43,14 @@ def admit(pending_bytes, free_bytes: int, max_batch: int, pending_samples=None, 
     return n
 
 
+def batch_cap(max_samples, queued_samples: int, workers: int, adaptive: bool):
+    """The sample cap of the next batch: max_samples, or, when adaptive and more waits than
+    the workers' share of it, an equal share of the queued samples per worker."""
+    if max_samples is None or not adaptive:
+        return max_samples
+    return max(max_samples, queued_samples // max(1, workers))
+
+
 @dataclass
 class _Pending:
     req: SearchRequest
@@ -54,12 +62,13 @@ class _Pending:
 
 class SearchServer:
     def __init__(self, hbm_budget_bytes: int = 120 << 30, workers: int = 2, max_batch: int = 64,
-                 input_bytes=None, max_batch_samples: Optional[int] = None):
+                 input_bytes=None, max_batch_samples: Optional[int] = None, adaptive_cap: bool = True):
         import torch
         self.budget = int(hbm_budget_bytes)
         self.used = 0
         self.max_batch = max_batch
         self.max_batch_samples = max_batch_samples
+        self.adaptive_cap = adaptive_cap
         self._input_bytes = input_bytes or (lambda r: r.input.numel() * r.input.element_size())
         self._q: deque = deque()
         self._cv = threading.Condition()
@@ -103,9 +112,14 @@ class SearchServer:
 
     def _take(self) -> List[_Pending]:
         """Pending requests, in arrival order, that fit the free budget (at most max_batch
-        requests and max_batch_samples samples)."""
+        requests and max_batch_samples samples).  When more work waits than the workers'
+        share of the sample cap, the cap grows to an equal share of the queue per worker: a
+        long queue is drained in large batches (throughput), a short one in small ones
+        (latency)."""
+        cap = batch_cap(self.max_batch_samples, sum(p.samples for p in self._q), len(self._threads),
+                        self.adaptive_cap)
         n = admit([p.bytes for p in self._q], self.budget - self.used, self.max_batch,
-                  [p.samples for p in self._q], self.max_batch_samples)
+                  [p.samples for p in self._q], cap)
         return [self._q.popleft() for _ in range(n)]
 
     def _work(self, stream):

@@ -18,6 +18,14 @@ def test_admission_takes_the_fitting_prefix():
     assert admit([1, 1], 100, 64, [10, 10], None) == 2
 
 
+def test_batch_cap_grows_with_the_queue():
+    from seticore_b200.serving import batch_cap
+    assert batch_cap(None, 10**9, 3, True) is None
+    assert batch_cap(100, 90, 3, True) == 100        # a short queue keeps the cap
+    assert batch_cap(100, 900, 3, True) == 300       # a long one is shared out per worker
+    assert batch_cap(100, 900, 3, False) == 100
+
+
 @pytest.mark.gpu
 def test_served_results_equal_results_alone():
     if not has_gpu():
