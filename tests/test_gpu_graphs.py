@@ -1,7 +1,8 @@
 """The engine replays a repeated batch from a captured CUDA graph (second sight: capture,
 later: replay).  A replay must behave exactly like a direct call: it reads the input buffer's
 current contents, reports the tree's time, and is not reused when a setting that changes the
-launches (exact statistics, the staging-wait limit, the storage form) or the scratch changes.
+launches (exact statistics, the staging-wait limit, the storage form, the 16-bit tree's form)
+or the scratch changes.
 """
 import numpy as np
 import pytest
@@ -63,4 +64,16 @@ def test_replayed_batches_match_direct_calls(torch_cuda, port_oracle):
         got16 = dd.search_batch_raw(buf, [-1, -1], [0, 1], s0.max_drift, 0.0, 8.0)
         assert dd.last_stats().precision == _capi.SC_DD_PRECISION_BF16
     assert [[(h.index, h.drift_steps) for h in r] for r in got16] == [[(h.index, h.drift_steps) for h in r] for r in got]
+    # and so is the 16-bit tree's form (paired FP16 or float accumulation): a replay captured
+    # with one form is not served to the other, and the hits stay the same
+    try:
+        assert L.sc_dd_set_paired_fp16(0) == _capi.SC_DD_OK
+        for _ in range(3):
+            flat = dd.search_batch_raw(buf, [-1, -1], [0, 1], s0.max_drift, 0.0, 8.0)
+            assert [[(h.index, h.drift_steps) for h in r] for r in flat] == \
+                [[(h.index, h.drift_steps) for h in r] for r in got]
+    finally:
+        L.sc_dd_set_paired_fp16(1)
+    again = dd.search_batch_raw(buf, [-1, -1], [0, 1], s0.max_drift, 0.0, 8.0)
+    assert [[(h.index, h.drift_steps) for h in r] for r in again] == [[(h.index, h.drift_steps) for h in r] for r in got]
     dd.close()
