@@ -85,8 +85,9 @@ ERROR_CASES = {
 @pytest.mark.parametrize("name", list(ERROR_CASES))
 def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle, name):
     """States the top-path-sum error of each form against the FP64 tree (printed as one JSON
-    line per case), and bounds it: FP32 1e-6, FP16 1e-3, BF16 1e-2 relative (to the top
-    sum), over the channels whose top is above the median top."""
+    line per case), and bounds it: FP32 1e-6, FP16 1e-3 (2e-3 for 16 and 32 rows, whose tree
+    adds in FP16: four or five levels of 2^-11), BF16 1e-2 relative (to the top sum), over the
+    channels whose top is above the median top."""
     import json
     from seticore_b200 import Dedopplerer
     from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
@@ -101,7 +102,7 @@ def test_path_sum_error_against_fp64_oracle(torch_cuda, port_oracle, name):
     top32 = dd.channel_array("top").cpu().numpy().astype(np.float64)
     sel = ref > np.percentile(ref, 50)  # the approximate tops are floored at 0 in normalised units
     err = {"fp32": float(np.max(np.abs(top32[sel] - ref[sel]) / ref[sel]))}
-    for prec, bound in (("fp16", 1e-3), ("bf16", 1e-2)):
+    for prec, bound in (("fp16", 2e-3 if c["T"] <= 32 else 1e-3), ("bf16", 1e-2)):
         dd.set_precision(prec)
         dd.search_raw(xt, -1, 0, spec.max_drift, 0.0, spec.snr_threshold)
         st = dd.last_stats()
