@@ -563,6 +563,9 @@ def main():
                                                   "(12*Tr*N + 20*N per search)",
                            "hits_identical_to_fp32": identical,
                            "recomputed_channels_first_search": f"{st.recomputed_channels}/{st.total_channels}",
+                           "tree_ms": float(np.median(ptree)) if ptree else None,
+                           "tree_note": "the 16-row tree launch (paired FP16: two drift blocks per __hadd2), "
+                                        "CUDA events on the launching stream",
                            "speedup_vs_fp32": ms / p_ms}
     dd.set_precision("fp32")
 
