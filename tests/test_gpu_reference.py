@@ -66,6 +66,29 @@ def test_node_coarse_channels_match_reference_gpu(torch_cuda, ref_gpu):
     assert total >= 16  # 4 tones + 2 spikes per coarse channel
 
 
+@pytest.mark.parametrize("precision", ["bf16", "fp16"])
+def test_16bit_forms_match_reference_gpu(torch_cuda, ref_gpu, precision):
+    """The 16-bit forms -- whose 16- and 32-row trees add FP16 pairs of two drift blocks --
+    against the reference's own GPU search: one node coarse channel (16 rows) and one 32-row
+    search of the uneven model."""
+    torch = torch_cuda
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import SearchSpec, config_node, make_filterbank_numpy
+    cases = [config_node(1, base_seed=2100)[0],
+             SearchSpec(32, 1 << 18, tsamp=18.253611 / 2, max_drift=3.0, seed=2101, n_tones=5, snr_threshold=10.0)]
+    for s in cases:
+        x = make_filterbank_numpy(s)
+        dd = Dedopplerer(s.num_timesteps, s.num_channels, s.foff_mhz, s.tsamp)
+        dd.set_precision(precision)
+        got = dd.search_raw(torch.from_numpy(x).cuda(), -1, 0, s.max_drift, s.min_drift, s.snr_threshold)
+        thr = dd.last_stats().threshold
+        dd.close()
+        want = ref_search(ref_gpu, x, s.num_timesteps, s.foff_mhz, s.tsamp, s.max_drift, s.min_drift, s.snr_threshold)
+        ties = compare_hits(as_dicts(got), want, thr, thr, f"{precision} T{s.num_timesteps}")
+        assert len(ties) <= 1, ties
+        assert len(want) >= 3
+
+
 def test_uneven_shapes_through_the_pool_match_reference_gpu(torch_cuda, ref_gpu):
     """64, 128 and 256 timesteps at 2^20 channels (the level path), mixed in one pool call."""
     torch = torch_cuda
