@@ -423,20 +423,39 @@ __device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem
   return (float)(lo - 0x1p-20 * (fabs(lo) + 1.0));
 }
 
+// Appends channel c to the flag list for every lane whose f holds (one atomic per warp).
+__device__ __forceinline__ void flag_append(const PrecisionDesc& d, bool f, int c) {
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if (m) {
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(d.flag_count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (f) d.flag_list[base + __popc(m & ((1u << lane) - 1u))] = c;
+  }
+}
+
+// Four channels per thread (16-byte loads) where the tops allow; the list's order does not
+// matter (each listed channel is recomputed on its own).
 __global__ void flag_channels_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
   const float thr_y = flag_threshold(d, b.elem);
-  const int lane = threadIdx.x & 31;
+  if (d.N % 4 == 0 && (reinterpret_cast<uintptr_t>(d.top16) & 15) == 0) {
+    const int n4 = d.N / 4;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n4; i0 += gridDim.x * blockDim.x) {
+      const int i = i0 + threadIdx.x;
+      const bool in = i < n4;
+      const float4 v = in ? __ldg(reinterpret_cast<const float4*>(d.top16) + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+      flag_append(d, in && !(v.x < thr_y), 4 * i);  // NaN is flagged
+      flag_append(d, in && !(v.y < thr_y), 4 * i + 1);
+      flag_append(d, in && !(v.z < thr_y), 4 * i + 2);
+      flag_append(d, in && !(v.w < thr_y), 4 * i + 3);
+    }
+    return;
+  }
   for (int c0 = blockIdx.x * blockDim.x; c0 < d.N; c0 += gridDim.x * blockDim.x) {
     const int c = c0 + threadIdx.x;
-    const bool f = c < d.N && !(d.top16[c] < thr_y);  // NaN is flagged
-    const unsigned m = __ballot_sync(0xffffffffu, f);
-    if (m) {
-      int base = 0;
-      if (lane == 0) base = atomicAdd(d.flag_count, __popc(m));
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (f) d.flag_list[base + __popc(m & ((1u << lane) - 1u))] = c;
-    }
+    flag_append(d, c < d.N && !(d.top16[c] < thr_y), c);  // NaN is flagged
   }
 }
 
@@ -554,8 +573,8 @@ cudaError_t normalize_batch(const PrecisionBatch& b, int num_sms, cudaStream_t s
 
 cudaError_t flag_channels_batch(const PrecisionBatch& b, int num_sms, cudaStream_t stream) {
   if (b.count <= 0) return cudaSuccess;
-  int blocks = (b.maxN + 255) / 256;
-  const int cap = (4 * num_sms + b.count - 1) / b.count;
+  int blocks = std::max(1, (b.maxN / 4 + 255) / 256);
+  const int cap = (16 * num_sms + b.count - 1) / b.count;
   if (blocks > cap) blocks = cap < 1 ? 1 : cap;
   flag_channels_kernel<<<dim3(blocks, b.count), 256, 0, stream>>>(b);
   return cudaGetLastError();
