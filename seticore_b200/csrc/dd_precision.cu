@@ -172,16 +172,23 @@ __device__ __forceinline__ __half from_float<__half>(float v) {
   return __float2half_rn(v);
 }
 
-// One read of the original power: y = (x - mean) / std in FP64, rounded to BF16 or FP16, into
-// the dense [Tr][N] 16-bit copy (padded rows 0); in the same read the float32 column sums in
+// The normalised value in float: (x - m) * inv with m = float(mean) and inv = float(1 / std),
+// each step rounded to nearest (no contraction).  The subtraction of two floats is exact or
+// off by 2^-24 of its result, so against (x - mean) / std the value carries a relative error
+// under 2^-22 (three roundings) and an absolute one of at most 1.01 * 2^-24 * |mean| / std
+// (the rounding of the mean): flag_threshold counts both.
+__device__ __forceinline__ float normalized(float x, float m, float inv) { return __fmul_rn(__fsub_rn(x, m), inv); }
+
+// One read of the original power: y = (x - mean) / std in float (normalized), rounded to BF16
+// or FP16, into the dense [Tr][N] 16-bit copy (padded rows 0); in the same read the float32 column sums in
 // row order (sumColumns, dedoppler.cu:63-72, bit-identical to colsum_kernel) and the minimum
 // and maximum of the unrounded rows, which the flag bound needs.  A thread takes four
 // columns (one with unaligned rows) down all Tr rows.
 template <typename E>
 __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
   const PrecisionDesc& d = b.s[blockIdx.y];
-  const double mean = d.moments[2 * kVarChunks];
-  const double inv = 1.0 / d.moments[2 * kVarChunks + 1];
+  const float mean = (float)d.moments[2 * kVarChunks];
+  const float inv = (float)(1.0 / d.moments[2 * kVarChunks + 1]);
   E* out = static_cast<E*>(d.norm);
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
@@ -198,10 +205,10 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
         cs.w += v.w;
         E y[4] = {from_float<E>(0.0f), from_float<E>(0.0f), from_float<E>(0.0f), from_float<E>(0.0f)};
         if (t < d.T) {
-          y[0] = from_float<E>((float)(((double)v.x - mean) * inv));
-          y[1] = from_float<E>((float)(((double)v.y - mean) * inv));
-          y[2] = from_float<E>((float)(((double)v.z - mean) * inv));
-          y[3] = from_float<E>((float)(((double)v.w - mean) * inv));
+          y[0] = from_float<E>(normalized(v.x, mean, inv));
+          y[1] = from_float<E>(normalized(v.y, mean, inv));
+          y[2] = from_float<E>(normalized(v.z, mean, inv));
+          y[3] = from_float<E>(normalized(v.w, mean, inv));
           mn = fminf(mn, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
           mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
         }
@@ -219,7 +226,7 @@ __global__ void normalize_kernel(const __grid_constant__ PrecisionBatch b) {
         cs += x;
         float y = 0.0f;
         if (t < d.T) {
-          y = (float)(((double)x - mean) * inv);
+          y = normalized(x, mean, inv);
           mn = fminf(mn, x);
           mx = fmaxf(mx, x);
         }
@@ -247,7 +254,7 @@ __device__ __forceinline__ unsigned short pair_bits(float y) {
 }
 
 // The paired copy of a 16- or 32-row search (the paired-FP16 tree's input): the same single
-// read as normalize_kernel -- y in FP64, rounded to the storage form, the float32 column sums
+// read as normalize_kernel -- y in float, rounded to the storage form, the float32 column sums
 // in row order and the extremes -- but it writes, for row t and channel x in [-kPairPad, N),
 // the word (y[t][x], y[t][x + t]) as two FP16 values (0 outside [0, N)): the leaves of drift
 // blocks k and k + 1 side by side, since the tree reads row t of drift block k + 1 t channels
@@ -262,8 +269,8 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
   // sixteen rows of kPairCols + kPairPad values (2112 bytes: every 4-value group is 8-byte
   // aligned)
   __shared__ __align__(16) unsigned short ys[16][kPairCols + kPairPad];
-  const double mean = d.moments[2 * kVarChunks];
-  const double inv = 1.0 / d.moments[2 * kVarChunks + 1];
+  const float mean = (float)d.moments[2 * kVarChunks];
+  const float inv = (float)(1.0 / d.moments[2 * kVarChunks + 1]);
   uint32_t* out = static_cast<uint32_t*>(d.norm);
   const long long np = ((long long)d.N + kPairPad + 3) / 4 * 4;  // pair_row_words(N)
   const int N = d.N, T = d.T;
@@ -285,7 +292,7 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
         const long long x = c0 + kPairCols + i;
         unsigned short hv = 0;
         if (x < N && g + u < T)
-          hv = pair_bits<E>((float)(((double)__ldg(d.input + (long long)(g + u) * d.row_stride + x) - mean) * inv));
+          hv = pair_bits<E>(normalized(__ldg(d.input + (long long)(g + u) * d.row_stride + x), mean, inv));
         ys[u][kPairCols + i] = hv;
       }
       // four channels per thread down the sixteen rows, eight rows' loads in flight at a
@@ -317,7 +324,7 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
               if (i < nin) {
-                packed |= (unsigned long long)pair_bits<E>((float)(((double)e[u][i] - mean) * inv)) << (16 * i);
+                packed |= (unsigned long long)pair_bits<E>(normalized(e[u][i], mean, inv)) << (16 * i);
                 mn = fminf(mn, e[u][i]);
                 mx = fmaxf(mx, e[u][i]);
               }
@@ -376,9 +383,11 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
 // top S~ (the 16-bit tree's) of at least this value, so it is listed and recomputed.
 //
 // Rounding bounds, per path of the T unrounded rows (padded rows are 0 on both sides):
-//  * y_i = (x_i - mean) / std in FP64, then to float and to 16 bits: |y~_i - y_i| <= u |y_i|
-//    with u = 2^-8 + 2^-24 (BF16; 2^-11 + 2^-24 for FP16, plus an absolute 2^-25 below
-//    FP16's normal range, which covers its subnormals and its flush to zero).
+//  * y_i = (x_i - mean) / std, formed in float (normalized: relative error under 2^-22,
+//    absolute 1.01 * 2^-24 * |mean| / std), then rounded to 16 bits:
+//    |y~_i - y_i| <= u |y_i| + e_abs with u = 2^-8 + 2^-22 (BF16; 2^-11 + 2^-22 for FP16) and
+//    e_abs = 1.01 * 2^-24 * |mean| / std, plus 2^-25 below FP16's normal range (its
+//    subnormals and its flush to zero).
 //  * float sums of n terms in the tree's pairwise order (depth L = log2 Tr): the error is
 //    at most g * sum|terms| with g = 1.01 L 2^-24, for both P_f and S~.
 //  * y_i >= -Ym with Ym = max(0, (mean - min x) / std), so sum|y_i| <= S_y + 2 T Ym along a
@@ -391,8 +400,8 @@ __global__ void __launch_bounds__(256, 4) normalize_pair_kernel(const __grid_con
 // The paired-FP16 tree (pair16) adds in FP16 instead: each add is off by at most 2^-11 of
 // its result or, below FP16's normal range, by 2^-25 absolute, so its sums are within
 // h sum|terms| + Tr 2^-25 (1.01) with h = 1.01 L 2^-11; BF16 leaves are rounded to FP16 on the
-// way (e_abs = 2^-25 for both forms).  Then S~ >= S_y - c (|S_y| + 2 T Ym) - T e_abs (1 + h)
-// - 1.01 Tr 2^-25 with c = u + h (1 + u).  No partial sum can overflow while Tr * ymax
+// way (its 2^-25 below FP16's normal range then applies to both forms).  Then
+// S~ >= S_y - c (|S_y| + 2 T Ym) - T e_abs (1 + h) - 1.01 Tr 2^-25 with c = u + h (1 + u).  No partial sum can overflow while Tr * ymax
 // stays below 60000 (FP16's largest value is 65504); beyond it every channel is listed.
 // A margin of 2^-20 relative guards the double arithmetic here; NaN inputs and NaN tops are
 // always listed.
@@ -405,8 +414,8 @@ __device__ __forceinline__ float flag_threshold(const PrecisionDesc& d, int elem
   const bool fp16 = (elem == kElemF16);
   const bool pair = d.pair16 != 0;
   const double h = pair ? 1.01 * L * 0x1p-11 : g;  // the 16-bit tree's own add bound
-  const double u = (fp16 ? 0x1p-11 : 0x1p-8) + 0x1p-24;
-  const double e_abs = (fp16 || pair) ? 0x1p-25 : 0.0;
+  const double u = (fp16 ? 0x1p-11 : 0x1p-8) + 0x1p-22;
+  const double e_abs = ((fp16 || pair) ? 0x1p-25 : 0.0) + 1.01 * 0x1p-24 * fabs(mean) / sd;
   const double T = (double)d.T;
   const double xn = xmin < 0.0 ? -xmin : 0.0;
   const double ym = fmax(0.0, (mean - xmin) / sd);

@@ -230,7 +230,8 @@ def test_paired_fp16_tree_equals_the_fp16_recursion(torch_cuda, precision, T):
     st = dd.last_stats()
     top16 = dd.channel_array("top16").cpu().numpy()
     assert got == want
-    y = (((x.astype(np.float64) - st.norm_mean) * (1.0 / st.norm_std)).astype(np.float32))
+    # the normalising pass's float arithmetic: (x - float(mean)) * float(1 / std), each step rounded
+    y = (x.astype(np.float32) - np.float32(st.norm_mean)) * np.float32(1.0 / st.norm_std)
     if precision == "bf16":
         y = _round_bf16(y)
     y16 = y.astype(np.float16)
