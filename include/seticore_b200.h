@@ -79,11 +79,12 @@ typedef struct sc_dd_stats {
 
 /* Storage of the spectra the tree reads.  FP32: the input as given (the reference's
  * form).  BF16 / FP16: each search first normalises its input per coarse channel,
- * (x - mean) / std with FP64 mean and std, into a 16-bit copy; the tree accumulates in
- * FP32 over that copy, every channel whose top could reach the threshold (its 16-bit top
- * reaches the threshold less a bound on the rounding of the 16-bit values and of the FP32
- * sums) is then recomputed in FP32 from the original power, and the hit list equals the
- * FP32 form's. */
+ * (x - mean) / std with an FP64 mean and std (the arithmetic in float), into a 16-bit copy;
+ * the tree accumulates in FP32 over that copy (for 16 and 32 rounded timesteps in FP16
+ * pairs of two drift blocks, see sc_dd_set_paired_fp16), every channel whose top could reach
+ * the threshold (its 16-bit top reaches the threshold less a bound on the rounding of the
+ * normalised values and of the tree's sums) is then recomputed in FP32 from the original
+ * power, and the hit list equals the FP32 form's. */
 enum { SC_DD_PRECISION_FP32 = 0, SC_DD_PRECISION_BF16 = 1, SC_DD_PRECISION_FP16 = 2 };
 
 typedef struct sc_dd sc_dd;
@@ -142,10 +143,10 @@ int sc_dd_add_incoherent_power(sc_dd* dd, const float* dev_input, long long row_
                                sc_dd_hit* hits, int num_hits, void* stream);
 
 /* Selects the storage form of later searches (SC_DD_PRECISION_*).  The 16-bit forms store
- * the FP64-normalised power as BF16 or FP16, sum it in FP32, and recompute in FP32, from
- * the original power, the top of every channel that the rounding bound cannot exclude
- * from the threshold, so their hit lists equal the FP32 form's.  They allocate their
- * scratch on first use. */
+ * the normalised power as BF16 or FP16, sum it (in FP32, or in FP16 pairs for 16 and 32
+ * rounded timesteps), and recompute in FP32, from the original power, the top of every
+ * channel that the rounding bound cannot exclude from the threshold, so their hit lists
+ * equal the FP32 form's.  They allocate their scratch on first use. */
 int sc_dd_set_precision(sc_dd* dd, int precision);
 
 /* Statistics of the first search of the engine's last completed call; tree_ms and
