@@ -610,7 +610,7 @@ int sc_dd_create(int num_timesteps, int num_channels, double foff_mhz, double ts
     // All pairs of level buffers in one allocation: the emitting level addresses a pair as
     // one array; pair 0 serves the main stream, pair 1 + i side stream i.
     const size_t L = scb::level_buffer_floats(d->Tr, num_channels);
-    const int sides = scb::level_sides();
+    const int sides = scb::level_sides(true);
     d->level_pairs = 1 + sides;
     if ((e = dalloc(d, &d->scratch_a, 2 * (size_t)d->level_pairs * sizeof(float) * L)) != cudaSuccess) {
       d->level_pairs = 1;

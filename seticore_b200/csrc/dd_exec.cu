@@ -122,13 +122,16 @@ TreeGroup tree_group(const ExecSearch& e, const void* rows, long long row_stride
 
 }  // namespace
 
-int level_sides() {
-  static const int v = [] {
+int level_sides(bool engine) {
+  static const long v = [] {
     const char* e = getenv("SETICORE_B200_LEVEL_SIDES");
-    const long x = e ? strtol(e, nullptr, 10) : 1;
-    return (int)std::min<long>(kLevelSides, std::max<long>(0, x));
+    return e ? strtol(e, nullptr, 10) : -1L;
   }();
-  return v;
+  // An engine holds one search shape, so its extra buffer pairs are small: three sides
+  // (beams 194.5 -> 197.4 Gsamples/s).  A pool sizes its pairs for its largest search and
+  // serves beside others: one.
+  const long x = v >= 0 ? v : (engine ? 3 : 1);
+  return (int)std::min<long>(kLevelSides, std::max<long>(0, x));
 }
 
 cudaError_t exec_queue(const ExecSearch* s, int n, float* lvl_a, float* lvl_b, int num_sms, cudaStream_t stream,

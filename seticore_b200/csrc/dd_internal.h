@@ -416,8 +416,9 @@ struct LevelSide {
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[kLevelSides] = {};
 };
-// Side streams an engine or pool creates (SETICORE_B200_LEVEL_SIDES, 0 to 3; default 1).
-int level_sides();
+// Side streams an engine (engine = true) or a pool creates: SETICORE_B200_LEVEL_SIDES, 0 to 3;
+// by default 3 for an engine and 1 for a pool.
+int level_sides(bool engine);
 
 // Queues every kernel of n searches (any mix) on `stream`; no synchronisation.
 // lvl_a / lvl_b: level buffers of level_buffer_floats(Tr, N) floats for every search with

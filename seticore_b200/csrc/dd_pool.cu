@@ -311,8 +311,8 @@ int sc_dd_pool_create(size_t scratch_budget_bytes, sc_dd_pool** out) {
   cudaError_t e = cudaGetDevice(&p->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess && scb::level_sides() > 0) e = cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming);
-  for (int i = 0; i < scb::level_sides() && e == cudaSuccess; ++i) {
+  if (e == cudaSuccess && scb::level_sides(false) > 0) e = cudaEventCreateWithFlags(&p->side.fork, cudaEventDisableTiming);
+  for (int i = 0; i < scb::level_sides(false) && e == cudaSuccess; ++i) {
     if ((e = cudaStreamCreateWithFlags(&p->side.stream[i], cudaStreamNonBlocking)) == cudaSuccess &&
         (e = cudaEventCreateWithFlags(&p->side.join[i], cudaEventDisableTiming)) == cudaSuccess)
       p->side.n = i + 1;
