@@ -30,7 +30,9 @@ CASES = [(16, 65536, 4.0, 1, 1), (16, 40000, 4.0, 2, 0), (8, 30000, 2.0, 3, 2), 
          (32, 65536, 4.0, 8, 1), (100, 32768, 2.0, 9, 0), (256, 131072, 2.0, 10, 1),
          # rows of a length that is not a whole number of 16-byte chunks: no bulk copy can take
          # them, so they are staged by per-thread loads
-         (16, 30001, 4.0, 11, 1), (32, 12345, 3.0, 12, 0)]
+         (16, 30001, 4.0, 11, 1), (32, 12345, 3.0, 12, 0),
+         # narrow bands: one block of channels, most strips at the band's edges
+         (16, 1000, 2.0, 13, 0), (32, 700, 2.0, 14, 0)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"T{c[0]}_N{c[1]}_s{c[3]}")
