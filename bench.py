@@ -354,7 +354,7 @@ def serve_result(world, rank, local, n_inputs, serve_seconds):
         points = []
         for load in [0.5, 0.8, 1.0, 1.2]:
             rate = load * cap_rps
-            n_req = int(min(4 * n_inputs, max(64, rate * serve_seconds)))
+            n_req = int(min(16 * n_inputs, max(64, rate * serve_seconds)))
             _, lat, wall, smp = run_load(lambda i: base[i % n_inputs], n_req, rate, server, seed=int(load * 100))
             slow = lat / alone[np.arange(n_req) % n_inputs]
             points.append({"offered_load": load, "rate_per_s": rate, "requests": n_req,
