@@ -77,3 +77,29 @@ def test_replayed_batches_match_direct_calls(torch_cuda, port_oracle):
     again = dd.search_batch_raw(buf, [-1, -1], [0, 1], s0.max_drift, 0.0, 8.0)
     assert [[(h.index, h.drift_steps) for h in r] for r in again] == [[(h.index, h.drift_steps) for h in r] for r in got]
     dd.close()
+
+
+def test_replayed_level_batches_match_direct_calls(torch_cuda, port_oracle):
+    """A batch of more than 32 rows deals its searches over the level side streams; captured
+    and replayed, the fork and join events hold them all in the graph and the results stay
+    those of a direct call (and of the oracle)."""
+    torch = torch_cuda
+    from seticore_b200 import Dedopplerer
+    from seticore_b200.synthetic import SearchSpec, make_filterbank_numpy
+    specs = [SearchSpec(64, 1 << 14, tsamp=18.253611 / 4, max_drift=2.0, seed=90 + i, n_tones=4,
+                        snr_threshold=8.0) for i in range(5)]
+    xs = [make_filterbank_numpy(s) for s in specs]
+    s0 = specs[0]
+    buf = [torch.from_numpy(x).cuda() for x in xs]
+    dd = Dedopplerer(64, 1 << 14, s0.foff_mhz, s0.tsamp)
+    runs = [dd.search_batch_raw(buf, [-1] * 5, list(range(5)), s0.max_drift, 0.0, 8.0) for _ in range(4)]
+    for r in runs[1:]:
+        assert [_keys(h) for h in r] == [_keys(h) for h in runs[0]]
+    for k in range(5):
+        want, _ = port_oracle.search(xs[k], s0.foff_mhz, s0.tsamp, s0.max_drift, 0.0, 8.0)
+        assert [(h.index, h.drift_steps) for h in runs[0][k]] == [(h["index"], h["drift_steps"]) for h in want]
+    # new contents in one buffer: the replay reads them
+    buf[2].copy_(torch.from_numpy(xs[4]).cuda())
+    got = dd.search_batch_raw(buf, [-1] * 5, list(range(5)), s0.max_drift, 0.0, 8.0)
+    assert _keys(got[2]) == _keys(runs[0][4])
+    dd.close()
